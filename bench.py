@@ -1,0 +1,361 @@
+#!/usr/bin/env python3
+"""Benchmark: PDHG iterations/s on the large power-law LP (one B200 per rank).
+
+Workload ("zipf_lp_2Mx5M"): m = 2,000,000 rows, n = 5,000,000 columns, row
+lengths Zipf(1.5) capped at 5000, uniform distinct columns, FP32 N(0,1) values
+times log-uniform row scales in [1e-2, 1e2], feasible by construction
+(seeded synthetic data; the actual nnz is reported).  One step = one PDHG
+iteration of the reference algorithm (A x̄ + dual update, Aᵀ y + primal
+update), inputs resident in HBM.  The CSR streams (~0.9 GB per product) are
+far larger than L2, so no flush is needed between steps.
+
+Lines printed (rank 0, one JSON line):
+  value      iterations/s over all ranks (replicas: every rank solves its own copy)
+  e2e        the same metric through pramaan_pdhg_solve() with pinned host
+             buffers: upload, 1000 iterations (checks every 100), download
+  roofline   the dominant product kernel's algorithmic bytes / CUDA-event time
+  cpu_baseline  the oracle's multi-threaded FP32 iteration on the host cores
+
+`--impl reference` times the reference algorithm's CPU restatement (the
+oracle; the reference has no CPU implementation of this path) on all host
+cores, for the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "pdhg_iterations_per_s"
+UNIT = "iterations/s"
+WORKLOAD = "zipf_lp_2Mx5M"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="pramaan_b200", choices=["pramaan_b200", "reference"])
+    p.add_argument("--m", type=int, default=2_000_000)
+    p.add_argument("--n", type=int, default=5_000_000)
+    p.add_argument("--cap", type=int, default=5000)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--e2e-iters", type=int, default=1000)
+    p.add_argument("--e2e-calls", type=int, default=3)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(args, nnz):
+    return {"workload": WORKLOAD, "m": args.m, "n": args.n, "nnz": int(nnz), "zipf_s": 1.5,
+            "row_len_cap": args.cap, "seed": args.seed, "step": "one PDHG iteration (reference algorithm)",
+            "l2": "inputs larger than L2 (CSR ~0.9 GB per product); no flush",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_tag: str):
+    """Per-launch DRAM bytes recorded from an ncu capture in profiles/."""
+    f = REPO / "profiles" / f"{kernel_tag}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(model, seconds: float):
+    """Oracle FP32 iteration on all host threads, on a bounded number of full
+    iterations of the same LP; returns (iterations/s, threads, sample text)."""
+    import ctypes as C
+
+    import oracle
+    from oracle import ptr
+
+    h = oracle.orc()
+    m, n = model.numRows(), model.numVars()
+    v32 = model.values.astype(np.float32)
+    order = np.argsort(model.col_idx, kind="stable")
+    rows = np.repeat(np.arange(m, dtype=np.int32), np.diff(model.row_ptr))
+    tci = rows[order].astype(np.int32)
+    tv = v32[order]
+    trp = np.zeros(n + 1, np.int32)
+    trp[1:] = np.cumsum(np.bincount(model.col_idx, minlength=n))
+    sig, tau = oracle.step_sizes(model)
+    c = model.obj_coeffs.astype(np.float32)
+    lr = model.row_lower.astype(np.float32)
+    ur = model.row_upper.astype(np.float32)
+    lx = model.var_lower.astype(np.float32)
+    ux = model.var_upper.astype(np.float32)
+    x = np.maximum(lx, np.minimum(0, ux)).astype(np.float32)
+    xb = x.copy()
+    y = np.zeros(m, np.float32)
+    args = [ptr(model.row_ptr), ptr(model.col_idx), ptr(v32), ptr(trp), ptr(tci), ptr(tv), ptr(sig),
+            ptr(lr), ptr(ur), ptr(tau), ptr(c), ptr(lx), ptr(ux), ptr(x), ptr(xb), ptr(y)]
+    threads = h.orc_num_threads()
+    t0 = time.perf_counter()
+    h.orc_pdhg_iterations_mt(m, n, *args, 1)
+    one = time.perf_counter() - t0
+    iters = max(1, int(seconds / max(one, 1e-6)))
+    t0 = time.perf_counter()
+    h.orc_pdhg_iterations_mt(m, n, *args, iters)
+    dt = time.perf_counter() - t0
+    return iters / dt, threads, f"{iters} full iterations of the same LP after 1 untimed ({dt:.1f} s)"
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from pramaan_b200.generators import zipf_lp
+
+    model = zipf_lp(args.m, args.n, cap=args.cap, seed=args.seed, device="cpu")
+    import oracle
+    from oracle import ptr
+
+    h = oracle.orc()
+    m, n = model.numRows(), model.numVars()
+    v32 = model.values.astype(np.float32)
+    order = np.argsort(model.col_idx, kind="stable")
+    rows = np.repeat(np.arange(m, dtype=np.int32), np.diff(model.row_ptr))
+    tci = rows[order].astype(np.int32)
+    tv = v32[order]
+    trp = np.zeros(n + 1, np.int32)
+    trp[1:] = np.cumsum(np.bincount(model.col_idx, minlength=n))
+    sig, tau = oracle.step_sizes(model)
+    c = model.obj_coeffs.astype(np.float32)
+    lr, ur = model.row_lower.astype(np.float32), model.row_upper.astype(np.float32)
+    lx, ux = model.var_lower.astype(np.float32), model.var_upper.astype(np.float32)
+    x = np.maximum(lx, np.minimum(0, ux)).astype(np.float32)
+    xb = x.copy()
+    y = np.zeros(m, np.float32)
+    a = [ptr(model.row_ptr), ptr(model.col_idx), ptr(v32), ptr(trp), ptr(tci), ptr(tv), ptr(sig),
+         ptr(lr), ptr(ur), ptr(tau), ptr(c), ptr(lx), ptr(ux), ptr(x), ptr(xb), ptr(y)]
+    for _ in range(args.warmup):
+        h.orc_pdhg_iterations_mt(m, n, *a, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h.orc_pdhg_iterations_mt(m, n, *a, 1)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    threads = h.orc_num_threads()
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, model.nnz()), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full iterations (the reference has no CPU PDHG; "
+                                       "its algorithm restated in C, OpenMP over rows/columns)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_gpu_arm(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import pramaan_b200
+    from pramaan_b200 import PdhgOptions, Session
+    from pramaan_b200.generators import model_from_tensors, zipf_lp
+
+    t = zipf_lp(args.m, args.n, cap=args.cap, seed=args.seed, device=f"cuda:{local}", as_tensors=True)
+    model = model_from_tensors(t)
+    del t
+    torch.cuda.empty_cache()
+    nnz = model.nnz()
+
+    opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True)
+    sess = Session(model, opts)
+    stream = torch.cuda.ExternalStream(sess.stream(), device=local)
+    for _ in range(args.warmup):
+        sess.iterate(1)
+    sess.synchronize()
+    sess.kernel_times(reset=True)
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sess.iterate(1)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        tt = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_dual, ms_primal, launches = sess.kernel_times(reset=True)
+    b_dual, b_primal = sess.kernel_bytes()
+    sess.close()
+    value = world * args.steps / (ms / 1000.0)
+
+    # dominant kernel roofline
+    hbm, peak_kind = measured_peaks()
+    kinds = [("spmv_dual_fused", ms_dual, b_dual), ("spmv_primal_fused", ms_primal, b_primal)]
+    tag, kms, kbytes = max(kinds, key=lambda k: k[1])
+    avg_s = kms / 1000.0 / args.steps
+    achieved = kbytes / avg_s / 1e9
+    roofline = {"bound": "hbm", "kernel": tag, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "traffic": ncu_traffic(f"{tag}_zipf_lp_2Mx5M"),
+                "algorithmic_bytes_per_launch": kbytes, "avg_launch_ms": avg_s * 1000}
+    other = [k for k in kinds if k[0] != tag][0]
+    roofline["other_kernel"] = {"kernel": other[0], "achieved": other[2] / (other[1] / 1000 / args.steps) / 1e9,
+                                "avg_launch_ms": other[1] / args.steps}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, nnz), "gpu_launches": int(launches),
+            "clocks": clk.summary(), "roofline": roofline}
+
+    # ---- end-to-end through the public C ABI with pinned host buffers ----
+    if not args.no_e2e:
+        pin = {}
+        for name in ("obj_coeffs", "row_ptr", "col_idx", "values", "row_lower", "row_upper",
+                     "var_lower", "var_upper"):
+            a = getattr(model, name)
+            tt = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+            tt.numpy()[...] = a
+            pin[name] = tt
+        from pramaan_b200.pdhg import ModelIR
+        pm = ModelIR(*(pin[k].numpy() for k in ("obj_coeffs", "row_ptr", "col_idx", "values",
+                                               "row_lower", "row_upper", "var_lower", "var_upper")),
+                     model.obj_sense, model.obj_offset)
+        solver = pramaan_b200.PdhgSolver(PdhgOptions(device=local, tolerance=0.0,
+                                                     max_iterations=args.e2e_iters, check_frequency=100))
+        solver.solve(pm)   # warm-up (module load, first-touch)
+        times = []
+        for _ in range(args.e2e_calls):
+            t0 = time.perf_counter()
+            r = solver.solve(pm)
+            times.append(time.perf_counter() - t0)
+        e2e_s = max(times) if world == 1 else max(times)
+        m, n = model.numRows(), model.numVars()
+        h2d = 4 * (m + 1) + 4 * nnz + 8 * nnz + 8 * n + 16 * m + 16 * n
+        d2h = 4 * n + 4 * m + 8 * m + 8 * 8 * (r.checks + 1)
+        line["e2e"] = {"value": world * args.e2e_iters / statistics.median(times), "unit": UNIT,
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "iterations_per_call": args.e2e_iters, "calls": args.e2e_calls,
+                       "call_s_median": statistics.median(times)}
+
+    if rank == 0 and not args.no_cpu_baseline:
+        v, threads, sample = cpu_baseline(model, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

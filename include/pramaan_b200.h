@@ -1,0 +1,175 @@
+/*
+ * pramaan_b200.h — C ABI of libpramaan_b200.so, the sm_100a restarted-PDHG LP
+ * solver that stands in for PRAMAAN's GPU PDHG path (src/gpu/).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns an int status (PRAMAAN_OK or a negative PRAMAAN_ERR_*).  The text of
+ * the last failure on the calling thread is available from
+ * pramaan_last_error(); for CUDA failures it has the reference's form
+ * "CUDA error in <file>:<line> - <message>" (src/gpu/cuda_utils.cuh:8-15).
+ * Solver outcomes (optimal, iteration limit, numerical failure) are reported
+ * through pramaan_solve_result.status and are never errors.
+ *
+ * Data types follow the reference's ModelIR (include/pramaan/ir.hpp:62-119)
+ * and CSRMatrix (include/pramaan/sparse_matrix.hpp:28-181): int32 indices,
+ * FP64 values, ranged rows row_lower <= A x <= row_upper, boxed variables,
+ * +-1e30 as "infinite".  All host arrays are owned by the caller, read during
+ * the call and never retained.
+ */
+#ifndef PRAMAAN_B200_H
+#define PRAMAAN_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PRAMAAN_API __attribute__((visibility("default")))
+#else
+#define PRAMAAN_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------- */
+#define PRAMAAN_OK 0
+#define PRAMAAN_ERR_INVALID_ARGUMENT (-1)
+#define PRAMAAN_ERR_CUDA (-2)
+#define PRAMAAN_ERR_DEVICE_TIMEOUT (-3)
+#define PRAMAAN_ERR_INTERNAL (-4)
+
+/* ---- solver status: values of pramaan::SolveStatus
+ *      (include/pramaan/simplex.hpp:26-33) ---------------------------------- */
+#define PRAMAAN_STATUS_OPTIMAL 0
+#define PRAMAAN_STATUS_INFEASIBLE 1
+#define PRAMAAN_STATUS_UNBOUNDED 2
+#define PRAMAAN_STATUS_ITERATION_LIMIT 3
+#define PRAMAAN_STATUS_NUMERICAL_FAILURE 4
+#define PRAMAAN_STATUS_WARM_START_REJECTED 5
+
+/* ---- objective sense (pramaan::ObjSense, include/pramaan/ir.hpp:28-31) --- */
+#define PRAMAAN_MINIMIZE 0
+#define PRAMAAN_MAXIMIZE 1
+
+/* ---- algorithm / termination selectors (extensions) --------------------- */
+#define PRAMAAN_ALGO_REFERENCE 0 /* the reference iteration, step sizes and restart rule */
+#define PRAMAAN_TERM_REFERENCE 0 /* abs. max primal violation, rel. max dual violation */
+
+/* LP in the reference's ModelIR form. */
+typedef struct pramaan_lp {
+    int32_t num_rows;          /* m                                            */
+    int32_t num_cols;          /* n                                            */
+    int32_t nnz;               /* row_ptr[m]                                   */
+    int32_t obj_sense;         /* PRAMAAN_MINIMIZE / PRAMAAN_MAXIMIZE          */
+    double obj_offset;         /* constant added to c^T x for reporting        */
+    const double* obj_coeffs;  /* [n]                                          */
+    const int32_t* row_ptr;    /* [m + 1]                                      */
+    const int32_t* col_idx;    /* [nnz]                                        */
+    const double* values;      /* [nnz]                                        */
+    const double* row_lower;   /* [m]                                          */
+    const double* row_upper;   /* [m]                                          */
+    const double* var_lower;   /* [n]                                          */
+    const double* var_upper;   /* [n]                                          */
+} pramaan_lp;
+
+/* Options.  The first three fields are pramaan::gpu::PdhgOptions
+ * (include/pramaan/gpu/pdhg_solver.hpp:9-13) with the same defaults; the rest
+ * are extensions whose defaults reproduce the reference behaviour. */
+typedef struct pramaan_pdhg_options {
+    double tolerance;         /* 1e-6                                          */
+    int32_t max_iterations;   /* 100000                                        */
+    int32_t check_frequency;  /* 100 (must be >= 1)                            */
+    int32_t algorithm;        /* PRAMAAN_ALGO_REFERENCE                        */
+    int32_t termination;      /* PRAMAAN_TERM_REFERENCE                        */
+    int32_t device;           /* CUDA device ordinal, default 0                */
+    int32_t use_graph;        /* 1: replay each check interval as a CUDA graph */
+    int32_t profile_kernels;  /* 1: time every product kernel with CUDA events */
+    int32_t reserved[7];
+} pramaan_pdhg_options;
+
+/* Result, mirroring pramaan::SolveResult (include/pramaan/simplex.hpp:40-76).
+ * x, row_activity and y are caller-owned output buffers (may be NULL). */
+typedef struct pramaan_solve_result {
+    int32_t status;            /* PRAMAAN_STATUS_*                              */
+    int32_t iterations;        /* = max_iterations when not optimal             */
+    double primal_residual;    /* reference criterion, FP64                     */
+    double dual_residual;      /* reference criterion, FP64                     */
+    double objective_value;    /* c^T x + obj_offset in the model's own sense   */
+    double* x;                 /* out [n]                                       */
+    double* row_activity;      /* out [m] = A x in FP64                         */
+    double* y;                 /* out [m], dual iterate (reference sign)        */
+    int32_t restarts;          /* restarts performed                            */
+    int32_t checks;            /* convergence checks performed                  */
+    double solve_ms;           /* wall time inside the call                     */
+    double reserved[6];
+} pramaan_solve_result;
+
+/* Library identification. */
+PRAMAAN_API const char* pramaan_version(void);
+/* Text of the last failure on the calling thread ("" when none). */
+PRAMAAN_API const char* pramaan_last_error(void);
+
+/* Fills *opt with the defaults listed above. */
+PRAMAAN_API void pramaan_pdhg_default_options(pramaan_pdhg_options* opt);
+
+/* One complete solve: replaces pramaan::gpu::PdhgSolver::solve
+ * (src/gpu/pdhg_solver.cu:169-411).  Uploads the LP, runs the PDHG loop on the
+ * GPU (FP32 iterates, FP64 residual checks on the device), and writes the
+ * result.  Returns PRAMAAN_OK when the solve ran (whatever its status). */
+PRAMAAN_API int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
+                       pramaan_solve_result* result);
+
+/* ---- test-harness launchers (src/gpu/pdhg.cu:77-241) --------------------- */
+
+/* y_out[m] = A x for the FP32 CSR (row_ptr[m+1], col_idx[nnz], values[nnz]),
+ * x[n].  Replaces launch_spmv (src/gpu/pdhg.cu:156-196).  m == 0 writes
+ * nothing. */
+PRAMAAN_API int pramaan_launch_spmv(const int32_t* row_ptr, const int32_t* col_idx, const float* values,
+                        int32_t nnz, const float* x, float* y_out, int32_t m, int32_t n);
+
+/* y_out[n] = A^T x for the same CSR, x[m].  Replaces launch_spmv_t
+ * (src/gpu/pdhg.cu:198-241); computed by a gather over a stored transpose
+ * (deterministic) instead of an atomic scatter.  m == 0 writes zeros. */
+PRAMAAN_API int pramaan_launch_spmv_t(const int32_t* row_ptr, const int32_t* col_idx, const float* values,
+                          int32_t nnz, const float* x, float* y_out, int32_t m, int32_t n);
+
+/* One Step-1 dense iteration, in place (src/gpu/pdhg.cu:77-146):
+ *   x <- max(0, x - tau * gradient)          (n entries)
+ *   y <- y + sigma * (Ax_bar - b)            (m entries) */
+PRAMAAN_API int pramaan_launch_pdhg_iteration(float* h_x, float* h_y, const float* h_gradient,
+                                  const float* h_Ax_bar, const float* h_b, int32_t n, int32_t m,
+                                  float tau, float sigma);
+
+/* ---- device-resident session (benchmarks and advanced callers) ----------- */
+
+typedef struct pramaan_pdhg_session pramaan_pdhg_session;
+
+/* Uploads the LP and prepares the iteration (step sizes, transpose, x0). */
+PRAMAAN_API int pramaan_session_create(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
+                           pramaan_pdhg_session** out);
+PRAMAAN_API int pramaan_session_destroy(pramaan_pdhg_session* s);
+/* Runs `iterations` PDHG iterations without convergence checks (asynchronous
+ * on the session stream; graph replay when use_graph is set). */
+PRAMAAN_API int pramaan_session_iterate(pramaan_pdhg_session* s, int32_t iterations);
+/* Waits for the session stream. */
+PRAMAAN_API int pramaan_session_synchronize(pramaan_pdhg_session* s);
+/* Reference FP64 residuals of the current iterate (synchronises). */
+PRAMAAN_API int pramaan_session_residuals(pramaan_pdhg_session* s, double* primal, double* dual);
+/* Copies the current FP32 iterates to host buffers (either may be NULL). */
+PRAMAAN_API int pramaan_session_get_iterates(pramaan_pdhg_session* s, float* x, float* y);
+/* The cudaStream_t the session launches on. */
+PRAMAAN_API void* pramaan_session_stream(pramaan_pdhg_session* s);
+/* Accumulated CUDA-event time (ms) and launch count of the two product
+ * kernels since the last reset (profile_kernels must be set; synchronises). */
+PRAMAAN_API int pramaan_session_kernel_times(pramaan_pdhg_session* s, double* ms_dual, double* ms_primal,
+                                 int64_t* launches, int32_t reset);
+/* Algorithmic bytes of one launch of each product kernel (see the layout
+ * notes in the library documentation). */
+PRAMAAN_API int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual,
+                                 double* bytes_primal);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRAMAAN_B200_H */

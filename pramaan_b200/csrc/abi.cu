@@ -1,0 +1,317 @@
+// abi.cu — the extern "C" boundary of libpramaan_b200.so.
+//
+// Every entry point catches C++ exceptions, records their text in a
+// thread-local buffer and returns a negative status, so no exception ever
+// crosses the C ABI.
+#include <chrono>
+#include <cstring>
+#include <cmath>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pdhg_engine.cuh"
+
+struct pramaan_pdhg_session {
+    std::unique_ptr<pb::PdhgEngine> eng;
+};
+
+namespace pb {
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& fn) {
+    try {
+        fn();
+        g_last_error.clear();
+        return PRAMAAN_OK;
+    } catch (const InvalidArgument& e) {
+        g_last_error = e.what();
+        return PRAMAAN_ERR_INVALID_ARGUMENT;
+    } catch (const DeviceTimeout& e) {
+        g_last_error = e.what();
+        return PRAMAAN_ERR_DEVICE_TIMEOUT;
+    } catch (const CudaError& e) {
+        g_last_error = e.what();
+        return PRAMAAN_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return PRAMAAN_ERR_INTERNAL;
+    } catch (...) {
+        g_last_error = "unknown exception";
+        return PRAMAAN_ERR_INTERNAL;
+    }
+}
+
+constexpr int kThreads = 256;
+
+// Step-1 dense iteration (src/gpu/pdhg.cu:42-66): nvcc contracts both
+// reference expressions to one FMA each; written explicitly here.
+__global__ void step1_kernel(float* __restrict__ x, const float* __restrict__ g, int n, float tau,
+                             float* __restrict__ y, const float* __restrict__ ax,
+                             const float* __restrict__ b, int m, float sigma) {
+    const int total = n > m ? n : m;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        if (i < n) x[i] = fmaxf(0.0f, __fmaf_rn(-tau, g[i], x[i]));
+        if (i < m) y[i] = __fmaf_rn(sigma, __fsub_rn(ax[i], b[i]), y[i]);
+    }
+}
+
+struct StreamHolder {
+    cudaStream_t st = nullptr;
+    StreamHolder() { PB_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)); }
+    ~StreamHolder() { if (st) cudaStreamDestroy(st); }
+};
+
+void check_flag(int* d_flag, cudaStream_t st) {
+    int h = 0;
+    PB_CUDA_CHECK(cudaMemcpyAsync(&h, d_flag, 4, cudaMemcpyDeviceToHost, st));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (h & 1) throw InvalidArgument("row_ptr must start at 0, be non-decreasing and end at nnz");
+    if (h & 2) throw InvalidArgument("col_idx entry out of bounds");
+}
+
+void spmv_harness(const int32_t* row_ptr, const int32_t* col_idx, const float* values, int nnz,
+                  const float* x, float* y_out, int m, int n, bool transpose) {
+    if (m < 0 || n < 0 || nnz < 0) throw InvalidArgument("negative dimension");
+    const int out_len = transpose ? n : m;
+    const int in_len = transpose ? m : n;
+    if (out_len == 0) return;
+    if (!y_out) throw InvalidArgument("y_out is NULL");
+    if (m > 0 && !row_ptr) throw InvalidArgument("row_ptr is NULL");
+    if (nnz > 0 && (!col_idx || !values)) throw InvalidArgument("col_idx/values is NULL");
+    if (in_len > 0 && nnz > 0 && !x) throw InvalidArgument("x is NULL");
+    StreamHolder sh;
+    cudaStream_t st = sh.st;
+    int dev = 0;
+    PB_CUDA_CHECK(cudaGetDevice(&dev));
+    DevBuf<int> flag(1);
+    PB_CUDA_CHECK(cudaMemsetAsync(flag.get(), 0, 4, st));
+    CsrDevice A;
+    static const int zero_rp = 0;
+    csr_upload_f32(A, m, n, nnz, m > 0 ? row_ptr : &zero_rp, col_idx, values, st, flag.get());
+    check_flag(flag.get(), st);
+    DevBuf<float> dx{size_t(in_len > 0 ? in_len : 1)}, dy{size_t(out_len)};
+    if (in_len > 0 && x)
+        PB_CUDA_CHECK(cudaMemcpyAsync(dx.get(), x, size_t(in_len) * 4, cudaMemcpyHostToDevice, st));
+    else
+        PB_CUDA_CHECK(cudaMemsetAsync(dx.get(), 0, dx.bytes(), st));
+    EpiStore<float, float> epi{dy.get()};
+    if (!transpose) {
+        SpmvLauncher<EpiStore<float, float>, float, float, false>::launch(A.view(false), dx.get(), epi,
+                                                                         flag.get(), st, dev);
+    } else {
+        CsrDevice AT;
+        csr_transpose(A, AT, st);
+        SpmvLauncher<EpiStore<float, float>, float, float, false>::launch(AT.view(false), dx.get(),
+                                                                         epi, flag.get(), st, dev);
+        PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    PB_CUDA_CHECK(cudaMemcpyAsync(y_out, dy.get(), size_t(out_len) * 4, cudaMemcpyDeviceToHost, st));
+    int h_status = 0;
+    PB_CUDA_CHECK(cudaMemcpyAsync(&h_status, flag.get(), 4, cudaMemcpyDeviceToHost, st));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (h_status & kDevErrTimeout) throw DeviceTimeout("device wait on a bulk copy exceeded its time limit");
+}
+
+pramaan_pdhg_options defaults() {
+    pramaan_pdhg_options o;
+    std::memset(&o, 0, sizeof(o));
+    o.tolerance = 1e-6;
+    o.max_iterations = 100000;
+    o.check_frequency = 100;
+    o.algorithm = PRAMAAN_ALGO_REFERENCE;
+    o.termination = PRAMAAN_TERM_REFERENCE;
+    o.device = 0;
+    o.use_graph = 1;
+    o.profile_kernels = 0;
+    return o;
+}
+
+}  // namespace
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" {
+
+const char* pramaan_version(void) { return "pramaan_b200 0.1.0 (sm_100a)"; }
+
+const char* pramaan_last_error(void) { return g_last_error.c_str(); }
+
+void pramaan_pdhg_default_options(pramaan_pdhg_options* opt) {
+    if (opt) *opt = defaults();
+}
+
+int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
+                       pramaan_solve_result* res) {
+    return guarded([&] {
+        if (!lp || !res) throw InvalidArgument("lp and result must not be NULL");
+        const pramaan_pdhg_options o = opt ? *opt : defaults();
+        const auto t0 = std::chrono::steady_clock::now();
+        res->status = PRAMAAN_STATUS_ITERATION_LIMIT;
+        res->iterations = 0;
+        res->restarts = 0;
+        res->checks = 0;
+        res->primal_residual = std::numeric_limits<double>::infinity();
+        res->dual_residual = std::numeric_limits<double>::infinity();
+        res->objective_value = 0.0;
+        validate_lp(*lp);
+        validate_options(o);
+        const int m = lp->num_rows, n = lp->num_cols;
+        // Trivial: no variables (src/gpu/pdhg_solver.cu:179-184).
+        if (n == 0) {
+            res->status = PRAMAAN_STATUS_OPTIMAL;
+            res->objective_value = lp->obj_offset;
+            if (res->row_activity)
+                for (int i = 0; i < m; ++i) res->row_activity[i] = 0.0;
+            res->solve_ms = 0.0;
+            return;
+        }
+        // Guard: NaN/Inf in the objective (src/gpu/pdhg_solver.cu:187-192).
+        for (int j = 0; j < n; ++j) {
+            if (!std::isfinite(lp->obj_coeffs[j])) {
+                res->status = PRAMAAN_STATUS_NUMERICAL_FAILURE;
+                res->solve_ms = 0.0;
+                return;
+            }
+        }
+        DeviceGuard g(o.device);
+        PdhgEngine eng(*lp, o);
+        eng.solve(*lp, res);
+        res->solve_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+int pramaan_launch_spmv(const int32_t* row_ptr, const int32_t* col_idx, const float* values,
+                        int32_t nnz, const float* x, float* y_out, int32_t m, int32_t n) {
+    return guarded([&] { spmv_harness(row_ptr, col_idx, values, nnz, x, y_out, m, n, false); });
+}
+
+int pramaan_launch_spmv_t(const int32_t* row_ptr, const int32_t* col_idx, const float* values,
+                          int32_t nnz, const float* x, float* y_out, int32_t m, int32_t n) {
+    return guarded([&] {
+        if (m == 0 && n > 0 && y_out)
+            for (int j = 0; j < n; ++j) y_out[j] = 0.0f;
+        if (m == 0) return;
+        spmv_harness(row_ptr, col_idx, values, nnz, x, y_out, m, n, true);
+    });
+}
+
+int pramaan_launch_pdhg_iteration(float* h_x, float* h_y, const float* h_gradient,
+                                  const float* h_Ax_bar, const float* h_b, int32_t n, int32_t m,
+                                  float tau, float sigma) {
+    return guarded([&] {
+        if (n <= 0 && m <= 0) return;
+        if (n < 0) n = 0;
+        if (m < 0) m = 0;
+        if (n > 0 && (!h_x || !h_gradient)) throw InvalidArgument("x/gradient is NULL");
+        if (m > 0 && (!h_y || !h_Ax_bar || !h_b)) throw InvalidArgument("y/Ax_bar/b is NULL");
+        StreamHolder sh;
+        cudaStream_t st = sh.st;
+        DevBuf<float> dx{size_t(n)}, dg{size_t(n)}, dy{size_t(m)}, dax{size_t(m)}, db{size_t(m)};
+        if (n > 0) {
+            PB_CUDA_CHECK(cudaMemcpyAsync(dx.get(), h_x, size_t(n) * 4, cudaMemcpyHostToDevice, st));
+            PB_CUDA_CHECK(cudaMemcpyAsync(dg.get(), h_gradient, size_t(n) * 4, cudaMemcpyHostToDevice, st));
+        }
+        if (m > 0) {
+            PB_CUDA_CHECK(cudaMemcpyAsync(dy.get(), h_y, size_t(m) * 4, cudaMemcpyHostToDevice, st));
+            PB_CUDA_CHECK(cudaMemcpyAsync(dax.get(), h_Ax_bar, size_t(m) * 4, cudaMemcpyHostToDevice, st));
+            PB_CUDA_CHECK(cudaMemcpyAsync(db.get(), h_b, size_t(m) * 4, cudaMemcpyHostToDevice, st));
+        }
+        const int total = n > m ? n : m;
+        const int grid = (total + kThreads - 1) / kThreads;
+        step1_kernel<<<grid, kThreads, 0, st>>>(dx.get(), dg.get(), n, tau, dy.get(), dax.get(),
+                                                 db.get(), m, sigma);
+        PB_CUDA_CHECK(cudaGetLastError());
+        if (n > 0) PB_CUDA_CHECK(cudaMemcpyAsync(h_x, dx.get(), size_t(n) * 4, cudaMemcpyDeviceToHost, st));
+        if (m > 0) PB_CUDA_CHECK(cudaMemcpyAsync(h_y, dy.get(), size_t(m) * 4, cudaMemcpyDeviceToHost, st));
+        PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    });
+}
+
+int pramaan_session_create(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
+                           pramaan_pdhg_session** out) {
+    return guarded([&] {
+        if (!lp || !out) throw InvalidArgument("lp and out must not be NULL");
+        *out = nullptr;
+        const pramaan_pdhg_options o = opt ? *opt : defaults();
+        DeviceGuard g(o.device);
+        auto s = std::make_unique<pramaan_pdhg_session>();
+        s->eng = std::make_unique<PdhgEngine>(*lp, o);
+        *out = s.release();
+    });
+}
+
+int pramaan_session_destroy(pramaan_pdhg_session* s) {
+    return guarded([&] {
+        if (!s) return;
+        DeviceGuard g(s->eng->device());
+        delete s;
+    });
+}
+
+int pramaan_session_iterate(pramaan_pdhg_session* s, int32_t iterations) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        DeviceGuard g(s->eng->device());
+        s->eng->iterate(iterations);
+    });
+}
+
+int pramaan_session_synchronize(pramaan_pdhg_session* s) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        DeviceGuard g(s->eng->device());
+        s->eng->synchronize();
+    });
+}
+
+int pramaan_session_residuals(pramaan_pdhg_session* s, double* primal, double* dual) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        DeviceGuard g(s->eng->device());
+        double pv = 0, dv = 0;
+        bool nf = false;
+        s->eng->residuals(pv, dv, nf);
+        if (primal) *primal = nf ? std::numeric_limits<double>::quiet_NaN() : pv;
+        if (dual) *dual = nf ? std::numeric_limits<double>::quiet_NaN() : dv;
+    });
+}
+
+int pramaan_session_get_iterates(pramaan_pdhg_session* s, float* x, float* y) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        DeviceGuard g(s->eng->device());
+        s->eng->get_iterates(x, y);
+    });
+}
+
+void* pramaan_session_stream(pramaan_pdhg_session* s) {
+    return s ? static_cast<void*>(s->eng->stream()) : nullptr;
+}
+
+int pramaan_session_kernel_times(pramaan_pdhg_session* s, double* ms_dual, double* ms_primal,
+                                 int64_t* launches, int32_t reset) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        DeviceGuard g(s->eng->device());
+        long long l = 0;
+        s->eng->kernel_times(ms_dual, ms_primal, &l, reset != 0);
+        if (launches) *launches = l;
+    });
+}
+
+int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual, double* bytes_primal) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        if (bytes_dual) *bytes_dual = s->eng->bytes_dual();
+        if (bytes_primal) *bytes_primal = s->eng->bytes_primal();
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// pdhg_engine.cuh — device-resident PDHG state and the host driver loop.
+#pragma once
+
+#include <vector>
+
+#include "csr_device.cuh"
+#include "epilogues.cuh"
+
+namespace pb {
+
+// Makes `dev` current for the lifetime of the guard and restores the
+// caller's device afterwards.
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int dev) {
+        PB_CUDA_CHECK(cudaGetDevice(&prev_));
+        if (dev != prev_) PB_CUDA_CHECK(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() { cudaSetDevice(prev_); }
+
+private:
+    int prev_ = 0;
+};
+
+void validate_lp(const pramaan_lp& lp);
+void validate_options(const pramaan_pdhg_options& opt);
+
+class PdhgEngine {
+public:
+    PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt);
+    ~PdhgEngine();
+    PdhgEngine(const PdhgEngine&) = delete;
+    PdhgEngine& operator=(const PdhgEngine&) = delete;
+
+    int device() const { return dev_; }
+    cudaStream_t stream() const { return st_; }
+    int rows() const { return m_; }
+    int cols() const { return n_; }
+
+    // `k` reference iterations, asynchronous.
+    void iterate(int k);
+    // Reference FP64 residuals of the current iterate (synchronises).
+    void residuals(double& pv, double& dv, bool& nonfinite);
+    // Reference restart: y <- 0, x̄ <- x.
+    void restart();
+    void get_iterates(float* h_x, float* h_y);
+    // Full solve loop (src/gpu/pdhg_solver.cu:319-410 semantics).
+    void solve(const pramaan_lp& lp, pramaan_solve_result* res);
+
+    void kernel_times(double* ms_dual, double* ms_primal, long long* launches, bool reset);
+    double bytes_dual() const;
+    double bytes_primal() const;
+    void synchronize();
+
+private:
+    void iterate_once();
+    void launch_dual();
+    void launch_primal();
+    void check_device_status();
+    void build_graph(int k);
+    void drain_events();
+
+    int dev_ = 0;
+    cudaStream_t st_ = nullptr;
+    pramaan_pdhg_options opt_{};
+    int m_ = 0, n_ = 0;
+    double c_norm_ = 1.0;
+
+    CsrDevice A_, AT_;
+    DevBuf<float> c_, lr_, ur_, lx_, ux_, sigma_, tau_, x_, y_, xbar_;
+    DevBuf<double> rlo64_, rhi64_, vlo64_, vhi64_, slots_;
+    DevBuf<int> status_;
+    double* h_slots_ = nullptr;   // pinned
+    int* h_status_ = nullptr;     // pinned
+
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    int graph_iters_ = 0;
+
+    // kernel timing (profile_kernels)
+    struct EvPair { cudaEvent_t a, b; int kind; };
+    std::vector<EvPair> ev_pool_;
+    size_t ev_used_ = 0;
+    double ms_dual_ = 0.0, ms_primal_ = 0.0;
+    long long launches_ = 0;
+};
+
+}  // namespace pb

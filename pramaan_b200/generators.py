@@ -1,0 +1,149 @@
+"""Seeded synthetic LP generators with the shapes of the benchmark configs.
+
+All generators build feasible LPs by construction (x0 feasible, and
+(y0, s0 >= 0) dual feasible):  min c^T x  s.t.  A x = b,  0 <= x <= u  with
+x0 ~ U(0,1), b = A x0, y0 ~ N(0,1), s0 ~ U(0,1), c = A^T y0 + s0,
+u = x0 + U(1,5).  Matrix values are FP32-representable numbers stored as
+FP64 (the ModelIR value type).
+
+* ``random_sparse_lp``  — "4 non-zeros per column at uniform random rows,
+  values N(0,1)" (the 1000 x 3000 plain-PDHG workload; any size).
+* ``zipf_lp``           — power-law rows: lengths Zipf(s) capped, uniform
+  distinct columns, values N(0,1) times log-uniform row scales (the
+  2,000,000 x 5,000,000 SpMV-roofline workload; any size).  Runs in torch on
+  any device so the large instance is generated on the GPU in about a second.
+* ``ill_conditioned_lp`` — k non-zeros per column with log-uniform row and
+  column scales (the 200,000 x 500,000 precision-ladder workload).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .pdhg import ModelIR, ObjSense
+
+
+def _csr_from_coo(rows: np.ndarray, cols: np.ndarray, vals: np.ndarray, m: int):
+    order = np.lexsort((cols, rows))
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    counts = np.bincount(rows, minlength=m)
+    row_ptr = np.zeros(m + 1, np.int64)
+    np.cumsum(counts, out=row_ptr[1:])
+    return row_ptr.astype(np.int32), cols.astype(np.int32), vals
+
+
+def _distinct_rows_per_col(rng: np.random.Generator, m: int, n: int, k: int) -> np.ndarray:
+    """(n, k) array of row indices, distinct within each column."""
+    k = min(k, m)
+    r = rng.integers(0, m, size=(n, k))
+    while True:
+        s = np.sort(r, axis=1)
+        dup_cols = np.nonzero((s[:, 1:] == s[:, :-1]).any(axis=1))[0]
+        if dup_cols.size == 0:
+            return r
+        r[dup_cols] = rng.integers(0, m, size=(dup_cols.size, k))
+
+
+def _feasible_model(rng, m, n, row_ptr, col_idx, vals) -> tuple[ModelIR, dict]:
+    rows = np.repeat(np.arange(m), np.diff(row_ptr))
+    x0 = rng.random(n)
+    b = np.bincount(rows, weights=vals * x0[col_idx], minlength=m)
+    y0 = rng.standard_normal(m)
+    s0 = rng.random(n)
+    c = np.bincount(col_idx, weights=vals * y0[rows], minlength=n) + s0
+    u = x0 + rng.uniform(1.0, 5.0, size=n)
+    model = ModelIR(c, row_ptr, col_idx, vals, b, b.copy(), np.zeros(n), u, ObjSense.kMinimize, 0.0)
+    return model, dict(x0=x0, y0=y0, s0=s0)
+
+
+def random_sparse_lp(m: int = 1000, n: int = 3000, nnz_per_col: int = 4, seed: int = 0,
+                     return_certificate: bool = False):
+    """Equality-constrained random sparse LP with k non-zeros per column."""
+    rng = np.random.default_rng(seed)
+    r = _distinct_rows_per_col(rng, m, n, nnz_per_col)
+    cols = np.repeat(np.arange(n), r.shape[1])
+    rows = r.reshape(-1)
+    vals = rng.standard_normal(rows.size).astype(np.float32).astype(np.float64)
+    row_ptr, col_idx, vals = _csr_from_coo(rows, cols, vals, m)
+    model, cert = _feasible_model(rng, m, n, row_ptr, col_idx, vals)
+    return (model, cert) if return_certificate else model
+
+
+def ill_conditioned_lp(m: int = 200_000, n: int = 500_000, nnz_per_col: int = 8, seed: int = 0,
+                       scale_exp: float = 4.0, return_certificate: bool = False):
+    """Random sparse LP with row and column scales log-uniform in
+    [10^-scale_exp, 10^scale_exp] (condition ~ 10^(4 scale_exp))."""
+    rng = np.random.default_rng(seed)
+    r = _distinct_rows_per_col(rng, m, n, nnz_per_col)
+    cols = np.repeat(np.arange(n), r.shape[1])
+    rows = r.reshape(-1)
+    rs = 10.0 ** rng.uniform(-scale_exp, scale_exp, size=m)
+    cs = 10.0 ** rng.uniform(-scale_exp, scale_exp, size=n)
+    vals = (rng.standard_normal(rows.size) * rs[rows] * cs[cols]).astype(np.float32).astype(np.float64)
+    row_ptr, col_idx, vals = _csr_from_coo(rows, cols, vals, m)
+    model, cert = _feasible_model(rng, m, n, row_ptr, col_idx, vals)
+    return (model, cert) if return_certificate else model
+
+
+def zipf_lp(m: int = 2_000_000, n: int = 5_000_000, s: float = 1.5, cap: int = 5000,
+            seed: int = 0, scale_lo: float = 1e-2, scale_hi: float = 1e2, device: str = "cpu",
+            as_tensors: bool = False):
+    """Power-law-row LP (torch on `device`).
+
+    Row lengths ~ Zipf(s) truncated to [1, cap]; columns uniform, distinct
+    within a row (duplicates drawn by chance are merged away, so the actual
+    nnz is reported by the result); values FP32(N(0,1) * row scale) with row
+    scales log-uniform in [scale_lo, scale_hi].  Returns a ModelIR (host) or,
+    with as_tensors=True, a dict of torch tensors on `device`.
+    """
+    import torch
+
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    cap = min(cap, n)
+    k = torch.arange(1, cap + 1, dtype=torch.float64, device=dev)
+    cdf = torch.cumsum(k.pow(-s), 0)
+    cdf = cdf / cdf[-1]
+    u = torch.rand(m, generator=g, dtype=torch.float64, device=dev)
+    lens = (torch.searchsorted(cdf, u) + 1).clamp_(1, cap)
+    rows = torch.repeat_interleave(torch.arange(m, device=dev), lens)
+    cols = torch.randint(0, n, (rows.numel(),), generator=g, device=dev)
+    key = rows * n + cols
+    del rows, cols
+    key, _ = torch.sort(key)
+    keep = torch.ones_like(key, dtype=torch.bool)
+    keep[1:] = key[1:] != key[:-1]
+    key = key[keep]
+    del keep
+    rows = torch.div(key, n, rounding_mode="floor")
+    cols = (key - rows * n).to(torch.int32)
+    del key
+    nnz = cols.numel()
+    counts = torch.bincount(rows, minlength=m)
+    row_ptr = torch.zeros(m + 1, dtype=torch.int64, device=dev)
+    torch.cumsum(counts, 0, out=row_ptr[1:])
+    lo, hi = np.log10(scale_lo), np.log10(scale_hi)
+    rscale = torch.pow(10.0, lo + (hi - lo) * torch.rand(m, generator=g, dtype=torch.float64, device=dev))
+    vals = (torch.randn(nnz, generator=g, dtype=torch.float64, device=dev) * rscale[rows]).float().double()
+    x0 = torch.rand(n, generator=g, dtype=torch.float64, device=dev)
+    b = torch.zeros(m, dtype=torch.float64, device=dev).index_add_(0, rows, vals * x0[cols.long()])
+    y0 = torch.randn(m, generator=g, dtype=torch.float64, device=dev)
+    s0 = torch.rand(n, generator=g, dtype=torch.float64, device=dev)
+    c = torch.zeros(n, dtype=torch.float64, device=dev).index_add_(0, cols.long(), vals * y0[rows]) + s0
+    del rows
+    ub = x0 + 1.0 + 4.0 * torch.rand(n, generator=g, dtype=torch.float64, device=dev)
+    t = dict(row_ptr=row_ptr.to(torch.int32), col_idx=cols, values=vals, obj_coeffs=c,
+             row_lower=b, row_upper=b.clone(), var_lower=torch.zeros(n, dtype=torch.float64, device=dev),
+             var_upper=ub, x0=x0, y0=y0, s0=s0)
+    if as_tensors:
+        return t
+    h = {k2: v.cpu().numpy() for k2, v in t.items()}
+    return ModelIR(h["obj_coeffs"], h["row_ptr"], h["col_idx"], h["values"], h["row_lower"],
+                   h["row_upper"], h["var_lower"], h["var_upper"], ObjSense.kMinimize, 0.0)
+
+
+def model_from_tensors(t: dict) -> ModelIR:
+    h = {k: v.cpu().numpy() for k, v in t.items() if k in (
+        "obj_coeffs", "row_ptr", "col_idx", "values", "row_lower", "row_upper", "var_lower", "var_upper")}
+    return ModelIR(h["obj_coeffs"], h["row_ptr"], h["col_idx"], h["values"], h["row_lower"],
+                   h["row_upper"], h["var_lower"], h["var_upper"], ObjSense.kMinimize, 0.0)
