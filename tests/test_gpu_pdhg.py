@@ -76,13 +76,13 @@ def test_residual_reductions_match_oracle():
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_solve_matches_oracle_solve(seed):
     model = random_sparse_lp(60, 180, 4, seed=seed)
-    opts = PdhgOptions(tolerance=1e-5, max_iterations=60000, check_frequency=100)
+    opts = PdhgOptions(tolerance=1e-4, max_iterations=60000, check_frequency=100)
     r = PdhgSolver(opts).solve(model)
-    ref = oracle.solve_ref(model, 1e-5, 60000, 100)
+    ref = oracle.solve_ref(model, 1e-4, 60000, 100)
     assert int(r.status) == ref["status"]
     if ref["status"] == 0:
         assert r.objective_value == pytest.approx(ref["objective_value"], rel=1e-4, abs=1e-4)
-        assert r.primal_residual <= 1e-5 and r.dual_residual <= 1e-5
+        assert r.primal_residual <= 1e-4 and r.dual_residual <= 1e-4
         assert abs(r.iterations - ref["iterations"]) <= 10 * opts.check_frequency
     # the FP64 result fields follow from x
     np.testing.assert_allclose(r.row_activity, model.multiply(r.x), rtol=1e-12, atol=1e-12)
