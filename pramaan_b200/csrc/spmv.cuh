@@ -278,7 +278,10 @@ __global__ void __launch_bounds__(BLOCK)
             if (rpb[head_row] >= tile_base) epi.apply(est, head_row, tot);
             else cross_tile(head_row, tot, false);
         }
-        if (tid == BLOCK - 1 && krow < m && rpb[krow + 1] > tile_end) {
+        // The tile's last row continues into the next tile: a piece of it
+        // lies in this tile only when the row starts before tile_end (a row
+        // starting exactly on the boundary belongs wholly to later tiles).
+        if (tid == BLOCK - 1 && krow < m && rpb[krow] < tile_end && rpb[krow + 1] > tile_end) {
             cross_tile(krow, kval, rpb[krow] >= tile_base);
         }
         __syncthreads();   // stage s, s_rp and s_w* free for reuse
