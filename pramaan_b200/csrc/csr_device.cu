@@ -1,8 +1,9 @@
-// csr_device.cu — uploads, FP32 hi/lo split, tile schedule and the on-device
-// stable transpose for CsrDevice.
+// csr_device.cu — uploads, FP32 hi/lo split, tiled-format construction and
+// the on-device stable transpose for CsrDevice.
 #include "csr_device.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 namespace pb {
 
@@ -26,35 +27,16 @@ inline int grid_1d(long long n, int cap = 65535 * 8) {
     return int(g < cap ? g : cap);
 }
 
-// tile_row[t] = max r in [0, rows] with row_ptr[r] <= t*T (t in 1..tiles-1),
-// tile_row[0] = 0, tile_row[tiles] = rows.
-__global__ void tile_row_kernel(const int* __restrict__ row_ptr, int rows, int tiles, int T,
-                                int* __restrict__ tile_row) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= tiles; t += gridDim.x * blockDim.x) {
-        if (t == 0) { tile_row[0] = 0; continue; }
-        if (t == tiles) { tile_row[t] = rows; continue; }
-        const long long key = (long long)t * T;
-        int lo = 0, hi = rows;   // answer in [0, rows]; row_ptr[0] = 0 <= key
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (row_ptr[mid] <= key) lo = mid; else hi = mid - 1;
-        }
-        tile_row[t] = lo;
-    }
-}
-
-__global__ void fill_pad_kernel(int* __restrict__ row_ptr, int rows, int nnz_pad) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) row_ptr[rows + 1] = nnz_pad;
-}
+#define PB_GRID_STRIDE(i, n)                                                            \
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n);       \
+         i += (long long)gridDim.x * blockDim.x)
 
 // Structural validation (the invariants CSRMatrix::validate enforces,
 // include/pramaan/sparse_matrix.hpp:153-174).  Flag bit 1: row_ptr not monotone /
-// bad end; bit 2: column index out of range.
+// bad ends; bit 2: column index out of range.
 __global__ void validate_kernel(const int* __restrict__ row_ptr, const int* __restrict__ col,
                                 int rows, int cols, int nnz, int* __restrict__ flag) {
-    const long long total = (long long)rows + nnz + 1;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
+    PB_GRID_STRIDE(i, (long long)rows + nnz + 1) {
         if (i < rows) {
             if (row_ptr[i] > row_ptr[i + 1]) atomicOr(flag, 1);
         } else if (i == rows) {
@@ -66,17 +48,88 @@ __global__ void validate_kernel(const int* __restrict__ row_ptr, const int* __re
     }
 }
 
-// val64 -> (hi, lo) with hi = RN(v), lo = RN(v - hi); flag bit 4 when any lo != 0.
+// val64 -> (hi, lo): hi = RN(v), lo = RN(v - hi); *inexact = 1 when any lo != 0.
 __global__ void split_f64_kernel(const double* __restrict__ v, int nnz, float* __restrict__ hi,
                                  float* __restrict__ lo, int* __restrict__ inexact) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz;
-         k += (long long)gridDim.x * blockDim.x) {
+    PB_GRID_STRIDE(k, nnz) {
         const double d = v[k];
         const float h = __double2float_rn(d);
         const float l = __double2float_rn(d - static_cast<double>(h));
         hi[k] = h;
         lo[k] = l;
         if (l != 0.0f) *inexact = 1;
+    }
+}
+
+__global__ void nonempty_kernel(const int* __restrict__ row_ptr, int rows, int* __restrict__ ne) {
+    PB_GRID_STRIDE(r, rows) ne[r] = row_ptr[r + 1] > row_ptr[r] ? 1 : 0;
+}
+
+// Compacted row pointer (non-empty rows, then nnz and nnz_pad), row map and
+// the empty-row list.
+__global__ void compact_rows_kernel(const int* __restrict__ row_ptr, const int* __restrict__ ne,
+                                    const int* __restrict__ idx, int rows, int* __restrict__ rp_c,
+                                    int* __restrict__ row_map, int* __restrict__ empty_rows) {
+    PB_GRID_STRIDE(r, rows) {
+        const int c = idx[r];
+        if (ne[r]) {
+            rp_c[c] = row_ptr[r];
+            if (row_map) row_map[c] = static_cast<int>(r);
+        } else if (empty_rows) {
+            empty_rows[r - c] = static_cast<int>(r);
+        }
+    }
+}
+
+__global__ void rp_tail_kernel(int* __restrict__ rp_c, int rows_c, int nnz, int nnz_pad) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        rp_c[rows_c] = nnz;
+        rp_c[rows_c + 1] = nnz_pad;
+    }
+}
+
+// Row-start bitmap: one bit per entry at the first entry of every non-empty
+// row, and at nnz when padding follows (the virtual padding row).
+__global__ void flags_kernel(const int* __restrict__ rp_c, int rows_c, int nnz, int nnz_pad,
+                             uint32_t* __restrict__ flags) {
+    PB_GRID_STRIDE(c, (long long)rows_c + 1) {
+        int q;
+        if (c < rows_c) q = rp_c[c];
+        else if (nnz < nnz_pad) q = nnz;
+        else continue;
+        atomicOr(&flags[q >> 5], 1u << (q & 31));
+    }
+}
+
+// Index of the compacted row holding entry q (rows_c + 2 pointer entries).
+__device__ int row_of_entry(const int* __restrict__ rp_c, int rows_c, long long q) {
+    int lo = 0, hi = rows_c;   // answer in [0, rows_c] (rows_c = virtual padding row)
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (rp_c[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// meta[t] = {first_row, head_t0, tail_span, tail_continues}
+//   first_row      compacted row holding the tile's first entry
+//   head_t0        tile where that row begins, or -1 when it begins at this tile
+//   tail_continues 1 when the row holding the tile's last entry continues into
+//                  the next tile
+//   tail_span      when that row also begins in this tile: the number of tiles
+//                  it touches (the arrivals its counter waits for), else 0
+__global__ void meta_kernel(const int* __restrict__ rp_c, int rows_c, int tiles, int T,
+                            int4* __restrict__ meta) {
+    PB_GRID_STRIDE(t, tiles) {
+        const long long base = t * (long long)T, last = base + T - 1;
+        const int fr = row_of_entry(rp_c, rows_c, base);
+        const int fstart = rp_c[fr];
+        const int head_t0 = fstart < base ? int(fstart / T) : -1;
+        const int tr = row_of_entry(rp_c, rows_c, last);
+        const long long tend = rp_c[tr + 1];
+        const int cont = (tr < rows_c && tend > last + 1) ? 1 : 0;
+        const int span = (cont && rp_c[tr] >= base) ? int((tend - 1) / T - t + 1) : 0;
+        meta[t] = make_int4(fr, head_t0, span, cont);
     }
 }
 
@@ -93,16 +146,13 @@ __global__ void expand_rows_kernel(const int* __restrict__ row_ptr, int rows,
 }
 
 __global__ void iota_kernel(int* __restrict__ a, int n) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x)
-        a[k] = static_cast<int>(k);
+    PB_GRID_STRIDE(k, n) a[k] = static_cast<int>(k);
 }
 
 // AT.row_ptr[c] = number of entries with sorted key < c (lower bound).
 __global__ void keys_to_rowptr_kernel(const int* __restrict__ keys, int nnz, int cols,
                                       int* __restrict__ rp) {
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c <= cols;
-         c += (long long)gridDim.x * blockDim.x) {
+    PB_GRID_STRIDE(c, (long long)cols + 1) {
         int lo = 0, hi = nnz;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
@@ -116,8 +166,7 @@ __global__ void permute_kernel(const int* __restrict__ perm, const int* __restri
                                const float* __restrict__ val, const float* __restrict__ lo,
                                int nnz, int* __restrict__ t_col, float* __restrict__ t_val,
                                float* __restrict__ t_lo) {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz;
-         k += (long long)gridDim.x * blockDim.x) {
+    PB_GRID_STRIDE(k, nnz) {
         const int src = perm[k];
         t_col[k] = row_of[src];
         t_val[k] = val[src];
@@ -133,29 +182,69 @@ void CsrDevice::allocate(int rows_, int cols_, int nnz_, bool lo) {
     num_tiles = nnz > 0 ? ceil_div(nnz, kSpmvTile) : 0;
     nnz_pad = num_tiles * kSpmvTile;
     has_lo = lo;
-    row_ptr.alloc(size_t(rows) + 2);
+    row_ptr.alloc(size_t(rows) + 1);
     col.alloc(size_t(nnz_pad));
     val.alloc(size_t(nnz_pad));
     if (lo) val_lo.alloc(size_t(nnz_pad)); else val_lo.reset();
-    tile_row.alloc(size_t(num_tiles) + 1);
-    counter.alloc(size_t(num_tiles > 0 ? num_tiles : 1));
-    carry.alloc(size_t(2) * (num_tiles > 0 ? num_tiles : 1));
 }
 
 void CsrDevice::finalize(cudaStream_t st) {
-    fill_pad_kernel<<<1, 1, 0, st>>>(row_ptr.get(), rows, nnz_pad);
-    PB_CUDA_CHECK(cudaGetLastError());
     if (nnz_pad > nnz) {
         PB_CUDA_CHECK(cudaMemsetAsync(col.get() + nnz, 0, size_t(nnz_pad - nnz) * 4, st));
         PB_CUDA_CHECK(cudaMemsetAsync(val.get() + nnz, 0, size_t(nnz_pad - nnz) * 4, st));
         if (val_lo.get())
             PB_CUDA_CHECK(cudaMemsetAsync(val_lo.get() + nnz, 0, size_t(nnz_pad - nnz) * 4, st));
     }
-    tile_row_kernel<<<grid_1d(num_tiles + 1), kThreads, 0, st>>>(row_ptr.get(), rows, num_tiles,
-                                                                 kSpmvTile, tile_row.get());
+    // ---- compact the non-empty rows ----
+    DevBuf<int> ne(size_t(rows > 0 ? rows : 1)), idx(size_t(rows) + 1);
+    rows_c = 0;
+    if (rows > 0) {
+        nonempty_kernel<<<grid_1d(rows), kThreads, 0, st>>>(row_ptr.get(), rows, ne.get());
+        PB_CUDA_CHECK(cudaGetLastError());
+        size_t tb = 0;
+        PB_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tb, ne.get(), idx.get(), rows, st));
+        DevBuf<unsigned char> temp(tb > 0 ? tb : 1);
+        PB_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(temp.get(), tb, ne.get(), idx.get(), rows, st));
+        int last_idx = 0, last_ne = 0;
+        PB_CUDA_CHECK(cudaMemcpyAsync(&last_idx, idx.get() + rows - 1, 4, cudaMemcpyDeviceToHost, st));
+        PB_CUDA_CHECK(cudaMemcpyAsync(&last_ne, ne.get() + rows - 1, 4, cudaMemcpyDeviceToHost, st));
+        PB_CUDA_CHECK(cudaStreamSynchronize(st));
+        rows_c = last_idx + last_ne;
+    }
+    num_empty = rows - rows_c;
+    if (num_empty > 0) {
+        row_map.alloc(size_t(rows_c > 0 ? rows_c : 1));
+        empty_rows.alloc(size_t(num_empty));
+    } else {
+        row_map.reset();
+        empty_rows.reset();
+    }
+    DevBuf<int> rp_c(size_t(rows_c) + 2);
+    if (rows > 0) {
+        compact_rows_kernel<<<grid_1d(rows), kThreads, 0, st>>>(
+            row_ptr.get(), ne.get(), idx.get(), rows, rp_c.get(), num_empty > 0 ? row_map.get() : nullptr,
+            num_empty > 0 ? empty_rows.get() : nullptr);
+        PB_CUDA_CHECK(cudaGetLastError());
+    }
+    rp_tail_kernel<<<1, 1, 0, st>>>(rp_c.get(), rows_c, nnz, nnz_pad);
     PB_CUDA_CHECK(cudaGetLastError());
+
+    // ---- row-start bitmap and tile descriptors ----
+    flags.alloc(size_t(nnz_pad / 32 > 0 ? nnz_pad / 32 : 1));
+    meta.alloc(size_t(num_tiles > 0 ? num_tiles : 1));
+    PB_CUDA_CHECK(cudaMemsetAsync(flags.get(), 0, flags.bytes(), st));
+    if (num_tiles > 0) {
+        flags_kernel<<<grid_1d((long long)rows_c + 1), kThreads, 0, st>>>(rp_c.get(), rows_c, nnz,
+                                                                         nnz_pad, flags.get());
+        meta_kernel<<<grid_1d(num_tiles), kThreads, 0, st>>>(rp_c.get(), rows_c, num_tiles, kSpmvTile,
+                                                             meta.get());
+        PB_CUDA_CHECK(cudaGetLastError());
+    }
+    counter.alloc(size_t(num_tiles > 0 ? num_tiles : 1));
+    carry.alloc(size_t(2) * (num_tiles > 0 ? num_tiles : 1));
     reset_counters(st);
     PB_CUDA_CHECK(cudaMemsetAsync(carry.get(), 0, carry.bytes(), st));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));   // temporaries are freed on return
 }
 
 void CsrDevice::reset_counters(cudaStream_t st) {
@@ -176,10 +265,21 @@ static void upload_structure(CsrDevice& A, int rows, int cols, int nnz, const in
     }
 }
 
+// Reads the validation flag; throws before any structure-dependent kernel runs.
+static void check_structure(int* d_flag, cudaStream_t st) {
+    if (!d_flag) return;
+    int h = 0;
+    PB_CUDA_CHECK(cudaMemcpyAsync(&h, d_flag, 4, cudaMemcpyDeviceToHost, st));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (h & 1) throw InvalidArgument("row_ptr must start at 0, be non-decreasing and end at nnz");
+    if (h & 2) throw InvalidArgument("col_idx entry out of bounds");
+}
+
 void csr_upload_f64(CsrDevice& A, int rows, int cols, int nnz, const int* h_row_ptr,
                     const int* h_col, const double* h_val, cudaStream_t st, int* d_flag) {
     A.allocate(rows, cols, nnz, /*lo=*/true);
     upload_structure(A, rows, cols, nnz, h_row_ptr, h_col, st, d_flag);
+    check_structure(d_flag, st);
     if (nnz > 0) {
         DevBuf<double> v64{size_t(nnz)};
         DevBuf<int> inexact(1);
@@ -203,6 +303,7 @@ void csr_upload_f32(CsrDevice& A, int rows, int cols, int nnz, const int* h_row_
                     const int* h_col, const float* h_val, cudaStream_t st, int* d_flag) {
     A.allocate(rows, cols, nnz, /*lo=*/false);
     upload_structure(A, rows, cols, nnz, h_row_ptr, h_col, st, d_flag);
+    check_structure(d_flag, st);
     if (nnz > 0)
         PB_CUDA_CHECK(cudaMemcpyAsync(A.val.get(), h_val, size_t(nnz) * 4, cudaMemcpyHostToDevice, st));
     A.finalize(st);
@@ -216,35 +317,28 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st) {
         AT.finalize(st);
         return;
     }
-    DevBuf<int> row_of{size_t(nnz)}, keys_out{size_t(nnz)}, perm_in{size_t(nnz)},
-        perm_out{size_t(nnz)};
-    {
-        long long warps = A.rows;
-        long long threads = warps * 32;
-        expand_rows_kernel<<<grid_1d(threads), kThreads, 0, st>>>(A.row_ptr.get(), A.rows,
-                                                                 row_of.get());
-        PB_CUDA_CHECK(cudaGetLastError());
-        iota_kernel<<<grid_1d(nnz), kThreads, 0, st>>>(perm_in.get(), nnz);
-        PB_CUDA_CHECK(cudaGetLastError());
-    }
+    DevBuf<int> row_of{size_t(nnz)}, keys_out{size_t(nnz)}, perm_in{size_t(nnz)}, perm_out{size_t(nnz)};
+    expand_rows_kernel<<<grid_1d((long long)A.rows * 32), kThreads, 0, st>>>(A.row_ptr.get(), A.rows,
+                                                                            row_of.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    iota_kernel<<<grid_1d(nnz), kThreads, 0, st>>>(perm_in.get(), nnz);
+    PB_CUDA_CHECK(cudaGetLastError());
     int end_bit = 1;
     while (end_bit < 31 && (1LL << end_bit) < (long long)A.cols) ++end_bit;
     size_t temp_bytes = 0;
     PB_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, A.col.get(), keys_out.get(),
                                                   perm_in.get(), perm_out.get(), nnz, 0, end_bit, st));
     DevBuf<unsigned char> temp(temp_bytes > 0 ? temp_bytes : 1);
-    PB_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(temp.get(), temp_bytes, A.col.get(),
-                                                  keys_out.get(), perm_in.get(), perm_out.get(),
-                                                  nnz, 0, end_bit, st));
-    keys_to_rowptr_kernel<<<grid_1d((long long)A.cols + 1), kThreads, 0, st>>>(
-        keys_out.get(), nnz, A.cols, AT.row_ptr.get());
+    PB_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(temp.get(), temp_bytes, A.col.get(), keys_out.get(),
+                                                  perm_in.get(), perm_out.get(), nnz, 0, end_bit, st));
+    keys_to_rowptr_kernel<<<grid_1d((long long)A.cols + 1), kThreads, 0, st>>>(keys_out.get(), nnz,
+                                                                              A.cols, AT.row_ptr.get());
     PB_CUDA_CHECK(cudaGetLastError());
     permute_kernel<<<grid_1d(nnz), kThreads, 0, st>>>(
         perm_out.get(), row_of.get(), A.val.get(), A.has_lo ? A.val_lo.get() : nullptr, nnz,
         AT.col.get(), AT.val.get(), AT.has_lo ? AT.val_lo.get() : nullptr);
     PB_CUDA_CHECK(cudaGetLastError());
-    AT.finalize(st);
-    PB_CUDA_CHECK(cudaStreamSynchronize(st));   // temporaries are freed on return
+    AT.finalize(st);   // synchronises; temporaries are freed on return
 }
 
 }  // namespace pb

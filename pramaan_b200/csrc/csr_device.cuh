@@ -1,17 +1,21 @@
-// csr_device.cuh — device-resident CSR operands in the tiled layout consumed
-// by spmv_merge_kernel, plus the launch helpers.
+// csr_device.cuh — device-resident CSR operands in the tiled format consumed
+// by spmv_tile_kernel, plus the launch helpers.
 //
 // Layout in HBM (one operand; A and its stored transpose each get one):
-//   row_ptr  int32 [rows + 2]    row_ptr[rows + 1] = nnz_pad (virtual pad row)
-//   col      int32 [nnz_pad]     pad entries: col 0
-//   val      fp32  [nnz_pad]     value rounded to nearest FP32, pad 0
-//   val_lo   fp32  [nnz_pad]     FP32(value - val); only kept when some value
-//                                is not exactly representable in FP32
-//   tile_row int32 [tiles + 1]   row holding the first non-zero of each tile
-//   carry    f64   [2 * tiles]   cross-tile partials (scratch)
-//   counter  int32 [tiles]       cross-tile arrival counters (scratch, zero at rest)
-// Every array starts on a 256-byte boundary (cudaMalloc), and nnz_pad is a
-// multiple of the 2048-entry tile, so every tile's slabs are 16-byte aligned
+//   row_ptr    int32 [rows + 1]        the CSR row pointer as given
+//   col        int32 [nnz_pad]         pad entries: col 0
+//   val        fp32  [nnz_pad]         value rounded to nearest FP32, pad 0
+//   val_lo     fp32  [nnz_pad]         FP32(value - val), kept only when some
+//                                      value is not exactly representable
+//   flags      u32   [nnz_pad / 32]    bit q: entry q starts a non-empty row
+//   meta       int4  [tiles]           {first_row, head_t0, tail_span, tail_continues}
+//   row_map    int32 [rows_c]          original row of each non-empty row (only
+//                                      when empty rows exist)
+//   empty_rows int32 [rows - rows_c]   rows without entries
+//   carry      f64   [2 * tiles]       cross-tile partials (scratch)
+//   counter    int32 [tiles]           cross-tile arrival counters (scratch, zero at rest)
+// nnz_pad is a multiple of the tile (2048 entries), and every array starts on
+// a 256-byte boundary (cudaMalloc), so each tile's slabs are 16-byte aligned
 // for the bulk copies.
 #pragma once
 
@@ -63,42 +67,49 @@ private:
 class CsrDevice {
 public:
     int rows = 0, cols = 0, nnz = 0, nnz_pad = 0, num_tiles = 0;
+    int rows_c = 0, num_empty = 0;
     bool has_lo = false;
-    DevBuf<int> row_ptr, col, tile_row, counter;
+    DevBuf<int> row_ptr, col, row_map, empty_rows, counter;
     DevBuf<float> val, val_lo;
+    DevBuf<uint32_t> flags;
+    DevBuf<int4> meta;
     DevBuf<double> carry;
 
     CsrView view(bool with_lo) const {
         CsrView v;
         v.rows = rows; v.cols = cols; v.nnz = nnz; v.nnz_pad = nnz_pad; v.num_tiles = num_tiles;
-        v.row_ptr = row_ptr.get(); v.col = col.get(); v.val = val.get();
+        v.rows_c = rows_c; v.num_empty = num_empty;
+        v.col = col.get(); v.val = val.get();
         v.val_lo = (with_lo && has_lo) ? val_lo.get() : nullptr;
-        v.tile_row = tile_row.get(); v.carry = carry.get(); v.counter = counter.get();
+        v.flags = flags.get(); v.meta = meta.get();
+        v.row_map = row_map.get(); v.empty_rows = empty_rows.get();
+        v.carry = carry.get(); v.counter = counter.get();
         return v;
     }
 
     // Algorithmic bytes of one SpMV over this operand: 8 nnz (col + val) +
-    // 4 (rows + 1) (row_ptr) + 4 cols (gathered vector, counted once) + 4 rows
-    // (result).
+    // 4 (rows + 1) (row structure) + 4 cols (gathered vector, counted once) +
+    // 4 rows (result).
     double spmv_bytes() const {
         return 8.0 * nnz + 4.0 * (rows + 1) + 4.0 * cols + 4.0 * rows;
     }
 
     // Allocates the padded arrays for the given shape.
     void allocate(int rows_, int cols_, int nnz_, bool lo);
-    // Builds tile_row from row_ptr and zeroes the scratch arrays.
+    // Builds flags / meta / row compaction from row_ptr and zeroes the scratch.
     void finalize(cudaStream_t st);
     // Zeroes the cross-tile counters (after an aborted launch).
     void reset_counters(cudaStream_t st);
     size_t device_bytes() const {
-        return row_ptr.bytes() + col.bytes() + tile_row.bytes() + counter.bytes() + val.bytes() +
-               val_lo.bytes() + carry.bytes();
+        return row_ptr.bytes() + col.bytes() + row_map.bytes() + empty_rows.bytes() +
+               counter.bytes() + val.bytes() + val_lo.bytes() + flags.bytes() + meta.bytes() +
+               carry.bytes();
     }
 };
 
 // Uploads a host CSR with FP64 values (reference ModelIR layout) and splits
-// every value into FP32 hi + FP32 lo on the device.  `validate_flag` receives
-// a nonzero code when row_ptr is not monotone or a column index is out of range.
+// every value into FP32 hi + FP32 lo on the device.  `d_flag` receives a
+// nonzero code when row_ptr is not monotone or a column index is out of range.
 void csr_upload_f64(CsrDevice& A, int rows, int cols, int nnz, const int* h_row_ptr,
                     const int* h_col, const double* h_val, cudaStream_t st, int* d_flag);
 // Uploads a host CSR with FP32 values (test-harness launchers).
@@ -117,40 +128,58 @@ int device_sm_count(int dev);
 template <class Epi, typename AccT, typename XT, bool kLo>
 struct SpmvLauncher {
     using L = SpmvSmemLayout<kSpmvBlock, kSpmvIpt, kSpmvStages, kLo, AccT>;
+    template <bool kRowMap>
     static constexpr auto kernel() {
-        return &spmv_merge_kernel<Epi, AccT, XT, kLo, kSpmvBlock, kSpmvIpt, kSpmvStages>;
+        return &spmv_tile_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvBlock, kSpmvIpt, kSpmvStages>;
     }
-    // Blocks per SM for this instantiation (queried once per device).
-    static int blocks_per_sm(int dev) {
+    template <bool kRowMap>
+    static int blocks_per_sm_impl(int dev) {
         static std::atomic<int> cache[64];
         if (dev < 0 || dev >= 64) dev = 0;
         int v = cache[dev].load(std::memory_order_relaxed);
         if (v > 0) return v;
-        PB_CUDA_CHECK(cudaFuncSetAttribute(kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(L::bytes)));
+        PB_CUDA_CHECK(cudaFuncSetAttribute(kernel<kRowMap>(),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes)));
         int nb = 0;
-        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel(), kSpmvBlock,
+        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel<kRowMap>(), kSpmvBlock,
                                                                     L::bytes));
         if (nb < 1) nb = 1;
         cache[dev].store(nb, std::memory_order_relaxed);
         return nb;
     }
-    static int grid_for(const CsrView& A, int dev) {
-        const long long cap = (long long)blocks_per_sm(dev) * device_sm_count(dev);
-        return int(A.num_tiles < cap ? A.num_tiles : cap);
+    // Queries occupancy (and sets the shared-memory attribute) for both
+    // variants; call before any stream capture.
+    static int blocks_per_sm(int dev) {
+        blocks_per_sm_impl<true>(dev);
+        return blocks_per_sm_impl<false>(dev);
     }
     static void launch(const CsrView& A, const XT* x, const Epi& epi, int* dev_status,
                        cudaStream_t st, int dev) {
         if (A.rows <= 0) return;
-        if (A.num_tiles == 0) {
-            const int grid = (A.rows + 255) / 256 < 4096 ? (A.rows + 255) / 256 : 4096;
-            zero_rows_kernel<Epi, AccT><<<grid, 256, 0, st>>>(A.rows, epi);
+        if (A.num_tiles > 0) {
+            const bool mapped = A.row_map != nullptr;
+            const long long cap = (long long)(mapped ? blocks_per_sm_impl<true>(dev)
+                                                     : blocks_per_sm_impl<false>(dev)) *
+                                  device_sm_count(dev);
+            const int grid = int(A.num_tiles < cap ? A.num_tiles : cap);
+            if (mapped) {
+                auto k = kernel<true>();
+                k<<<grid, kSpmvBlock, L::bytes, st>>>(A, x, epi, dev_status);
+            } else {
+                auto k = kernel<false>();
+                k<<<grid, kSpmvBlock, L::bytes, st>>>(A, x, epi, dev_status);
+            }
             PB_CUDA_CHECK(cudaGetLastError());
-            return;
         }
-        const int grid = grid_for(A, dev);
-        kernel()<<<grid, kSpmvBlock, L::bytes, st>>>(A, x, epi, dev_status);
-        PB_CUDA_CHECK(cudaGetLastError());
+        if (A.num_empty > 0) {
+            const int grid = (A.num_empty + 255) / 256 < 4096 ? (A.num_empty + 255) / 256 : 4096;
+            empty_rows_kernel<Epi, AccT><<<grid, 256, 0, st>>>(A.num_empty, A.empty_rows, epi);
+            PB_CUDA_CHECK(cudaGetLastError());
+        }
+    }
+    // Kernels launched by one launch() call.
+    static int launches(const CsrView& A) {
+        return (A.rows > 0 && A.num_tiles > 0 ? 1 : 0) + (A.rows > 0 && A.num_empty > 0 ? 1 : 0);
     }
 };
 

@@ -17,6 +17,7 @@ struct EpiStore {
     OutT* __restrict__ y;
     using State = NoState;
     __device__ void init(State&) const {}
+    __device__ void prefetch(int) const {}
     __device__ void apply(State&, int r, AccT v) const { y[r] = static_cast<OutT>(v); }
     __device__ void finish(State&) const {}
 };
@@ -31,6 +32,9 @@ struct EpiDualRef {
     float* __restrict__ y;
     using State = NoState;
     __device__ void init(State&) const {}
+    __device__ void prefetch(int i) const {
+        prefetch_l2(sigma + i); prefetch_l2(l_r + i); prefetch_l2(u_r + i); prefetch_l2(y + i);
+    }
     __device__ void apply(State&, int i, float ax) const {
         const float sig = sigma[i];
         if (sig <= 0.0f) return;
@@ -55,6 +59,10 @@ struct EpiPrimalRef {
     float* __restrict__ x_bar;
     using State = NoState;
     __device__ void init(State&) const {}
+    __device__ void prefetch(int j) const {
+        prefetch_l2(tau + j); prefetch_l2(c + j); prefetch_l2(l_x + j); prefetch_l2(u_x + j);
+        prefetch_l2(x + j);
+    }
     __device__ void apply(State&, int j, float aty) const {
         const float x_prev = x[j];
         const float g = __fadd_rn(c[j], aty);
@@ -83,6 +91,7 @@ struct EpiRowViolRef {
     double* __restrict__ slots;
     struct State { double mx; bool bad; };
     __device__ void init(State& s) const { s.mx = 0.0; s.bad = false; }
+    __device__ void prefetch(int i) const { prefetch_l2(row_lo + i); prefetch_l2(row_hi + i); }
     __device__ void apply(State& s, int i, double act) const {
         if (!isfinite(act)) { s.bad = true; return; }
         const double lo = row_lo[i], hi = row_hi[i];
@@ -108,6 +117,9 @@ struct EpiColResidRef {
     double* __restrict__ slots;
     struct State { double bmx, dmx; bool bad; };
     __device__ void init(State& s) const { s.bmx = 0.0; s.dmx = 0.0; s.bad = false; }
+    __device__ void prefetch(int j) const {
+        prefetch_l2(x + j); prefetch_l2(c + j); prefetch_l2(var_lo + j); prefetch_l2(var_hi + j);
+    }
     __device__ void apply(State& s, int j, double aty) const {
         const double xd = static_cast<double>(x[j]);
         const double lo = var_lo[j], hi = var_hi[j];

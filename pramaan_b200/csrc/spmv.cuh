@@ -6,50 +6,60 @@
 // transpose product is run by the same kernel over a stored transpose, so
 // both products are gathers and both are deterministic run to run.
 //
-// Work decomposition
-//   The nnz array is cut into tiles of T = BLOCK*IPT consecutive non-zeros.
-//   A persistent grid (a multiple of the SM count) walks the tiles with a
-//   static stride.  One elected thread streams each tile's col/val slabs into
-//   a STAGES-deep shared-memory ring with 1-D TMA bulk copies
-//   (cp.async.bulk ... mbarrier::complete_tx, L2 evict_first) while the
-//   block works on earlier tiles.  Every thread owns IPT consecutive
-//   non-zeros of the tile; it gathers x[col], multiplies, and walks the row
-//   boundaries (row_ptr slice staged in shared memory).  Rows that end inside
-//   the thread are finished on the spot; the rest are combined by a
-//   segmented block scan (warp shuffles + one shared-memory pass), and rows
-//   that cross a tile boundary by a "last arriver" rule: each tile holding a
-//   piece of such a row stores its partial in carry[], fences, and bumps the
-//   row's counter; the tile that brings the counter to the number of pieces
-//   adds the partials in tile order and runs the epilogue.  No thread ever
-//   waits on another block, and the summation order is fixed, so results
-//   are bit-identical between runs.
+// Tiled operand format (built once per matrix, see csr_device.cu)
+//   The non-zeros are cut into tiles of T = BLOCK*IPT consecutive entries.
+//   Per tile, four slabs sit at 16-byte aligned offsets:
+//     col   int32[T]      column indices
+//     val   fp32 [T]      values (FP32-rounded)      [+ val_lo fp32[T]]
+//     flags u32 [T/32]    bit q set <=> entry q starts a row
+//     meta  int4          {first_row, head_t0, tail_span, tail_continues}
+//   Empty rows are compacted out (an optional row_map gives the original row
+//   of every compacted row; empty rows get their epilogue from a separate
+//   pass), and the padding after the last entry forms a virtual row that is
+//   never emitted.  Row ids therefore follow from the bitmap alone:
+//   row(q) = first_row + #starts in (0, q], and the kernel never reads
+//   row_ptr.
 //
-// Row ownership: row r is finished by the thread whose item range (k0, k1]
-// contains row_ptr[r+1] (row 0..: thread 0 of tile 0 also owns rows ending at
-// 0).  Empty rows are therefore covered without a separate pass.  The device
-// row_ptr carries one extra entry row_ptr[rows+1] = nnz_pad: the padding
-// items [nnz, nnz_pad) (col 0, val 0) belong to a virtual row `rows` that is
-// never emitted.
+// Schedule
+//   A persistent grid (a multiple of the SM count) walks the tiles with a
+//   static stride.  Thread 0 streams every tile's four slabs into a
+//   STAGES-deep shared-memory ring with 1-D TMA bulk copies
+//   (cp.async.bulk ... mbarrier::complete_tx, L2 evict_first) while the
+//   block works on earlier tiles; waits on the ring's mbarriers are bounded.
+//   Every thread owns IPT consecutive entries.  Row ids come from popcounts
+//   of the bitmap (warp shuffles, no block barrier), the epilogue's vectors
+//   for the rows a thread will finish are prefetched into L2 together with
+//   the x gathers, and one segmented block scan (shuffles + one barrier)
+//   carries open-row partial sums across threads.  A row that crosses tile
+//   boundaries is finished by the "last arriver": each tile holding a piece
+//   stores its partial in carry[], bumps the row's counter with an acq_rel
+//   atomic, and the tile that completes the count adds the pieces in tile
+//   order.  No block ever waits on another block, and every sum has a fixed
+//   order, so results are bit-identical between runs.
 #pragma once
 
 #include "common.cuh"
 
 namespace pb {
 
-// Device view of one CSR operand in the tiled layout.
+// Device view of one CSR operand in the tiled format.
 struct CsrView {
-    int rows = 0, cols = 0;
+    int rows = 0;          // original rows (epilogue index space)
+    int cols = 0;
     int nnz = 0, nnz_pad = 0, num_tiles = 0;
-    const int* row_ptr = nullptr;    // rows + 2 entries
+    int rows_c = 0;        // non-empty (compacted) rows
+    int num_empty = 0;     // rows without entries
     const int* col = nullptr;        // nnz_pad
-    const float* val = nullptr;      // nnz_pad, value rounded to FP32
-    const float* val_lo = nullptr;   // nnz_pad, FP32 of (value - val) or null
-    const int* tile_row = nullptr;   // num_tiles + 1
-    void* carry = nullptr;           // 2 * num_tiles accumulators (double-sized slots)
+    const float* val = nullptr;      // nnz_pad
+    const float* val_lo = nullptr;   // nnz_pad or null
+    const uint32_t* flags = nullptr; // nnz_pad / 32
+    const int4* meta = nullptr;      // num_tiles
+    const int* row_map = nullptr;    // rows_c (null: identity)
+    const int* empty_rows = nullptr; // num_empty
+    void* carry = nullptr;           // 2 * num_tiles accumulators (8-byte slots)
     int* counter = nullptr;          // num_tiles, zero between launches
 };
 
-// Default tile geometry: 256 threads x 8 non-zeros = 2048 non-zeros per tile.
 constexpr int kSpmvBlock = 256;
 constexpr int kSpmvIpt = 8;
 constexpr int kSpmvTile = kSpmvBlock * kSpmvIpt;
@@ -59,49 +69,87 @@ template <int BLOCK, int IPT, int STAGES, bool kLo, typename AccT>
 struct SpmvSmemLayout {
     static constexpr int T = BLOCK * IPT;
     static constexpr int NW = BLOCK / 32;
-    static constexpr int RP_CAP = T + 8;   // row_ptr slice capacity (entries)
     static constexpr int kArrays = kLo ? 3 : 2;
+    static constexpr size_t flag_bytes = size_t(T) / 8;
+    static constexpr size_t stage_bytes = size_t(T) * 4 * kArrays + flag_bytes + 16;
     static constexpr size_t off_col = 0;
     static constexpr size_t off_val = off_col + size_t(STAGES) * T * 4;
     static constexpr size_t off_lo = off_val + size_t(STAGES) * T * 4;
-    static constexpr size_t off_rp = off_val + size_t(STAGES) * T * 4 * (kArrays - 1);
-    static constexpr size_t off_bar = off_rp + size_t(RP_CAP) * 4;
-    static constexpr size_t off_wrow = off_bar + size_t(STAGES) * 8;
-    static constexpr size_t off_wval = off_wrow + size_t(NW) * 4 + 8;
-    static constexpr size_t bytes = ((off_wval + size_t(NW) * sizeof(AccT)) + 127) / 128 * 128;
-    static_assert(RP_CAP % 2 == 0, "mbarriers need 8-byte alignment");
+    static constexpr size_t off_flags = off_val + size_t(STAGES) * T * 4 * (kArrays - 1);
+    static constexpr size_t off_meta = off_flags + size_t(STAGES) * flag_bytes;
+    static constexpr size_t off_bar = off_meta + size_t(STAGES) * 16;
+    static constexpr size_t off_wf = off_bar + size_t(STAGES) * 8;
+    static constexpr size_t off_wv = off_wf + 8 * ((size_t(NW) * 4 + 7) / 8);
+    static constexpr size_t bytes = ((off_wv + size_t(NW) * sizeof(AccT)) + 127) / 128 * 128;
+    static constexpr unsigned tx_bytes = unsigned(stage_bytes);
+    static_assert(T % 32 == 0 && 32 % IPT == 0, "IPT must divide 32");
+    static_assert((size_t(T) * 4) % 16 == 0 && flag_bytes % 16 == 0, "TMA slabs must be 16-byte multiples");
 };
 
 // Epilogue concept:
 //   struct Epi {
-//     struct State {...};                         // per-thread state
+//     struct State {...};                                  // per-thread state
 //     __device__ void init(State&) const;
+//     __device__ void prefetch(int row) const;             // L2 prefetch of row data
 //     __device__ void apply(State&, int row, AccT value) const;   // row complete
-//     __device__ void finish(State&) const;       // called once by every thread at exit
+//     __device__ void finish(State&) const;                // once by every thread at exit
 //   };
 
-template <class Epi, typename AccT, typename XT, bool kLo, int BLOCK, int IPT, int STAGES>
+__device__ __forceinline__ int atomic_add_acq_rel_gpu(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+template <typename T>
+__device__ __forceinline__ T ld_relaxed_gpu(const T* p);
+template <>
+__device__ __forceinline__ float ld_relaxed_gpu<float>(const float* p) {
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+template <>
+__device__ __forceinline__ double ld_relaxed_gpu<double>(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+template <typename AccT>
+struct SegPair {   // (row end seen, open-row partial)
+    int f;
+    AccT v;
+};
+
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int BLOCK, int IPT, int STAGES>
 __global__ void __launch_bounds__(BLOCK)
-    spmv_merge_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
-                      int* __restrict__ dev_status) {
+    spmv_tile_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
+                     int* __restrict__ dev_status) {
     using L = SpmvSmemLayout<BLOCK, IPT, STAGES, kLo, AccT>;
     constexpr int T = L::T;
     constexpr int NW = L::NW;
-    static_assert(IPT % 4 == 0, "IPT must allow 16-byte shared-memory vector reads");
+    constexpr int WPT = T / 32;              // flag words per tile
+    constexpr unsigned kMask = (IPT == 32) ? 0xffffffffu : ((1u << IPT) - 1u);
 
     extern __shared__ __align__(128) unsigned char smem[];
     int* s_col = reinterpret_cast<int*>(smem + L::off_col);
     float* s_val = reinterpret_cast<float*>(smem + L::off_val);
     float* s_lo = reinterpret_cast<float*>(smem + L::off_lo);
-    int* s_rp = reinterpret_cast<int*>(smem + L::off_rp);
+    uint32_t* s_flags = reinterpret_cast<uint32_t*>(smem + L::off_flags);
+    int4* s_meta = reinterpret_cast<int4*>(smem + L::off_meta);
     uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem + L::off_bar);
-    int* s_wrow = reinterpret_cast<int*>(smem + L::off_wrow);
-    AccT* s_wval = reinterpret_cast<AccT*>(smem + L::off_wval);
+    int* s_wf = reinterpret_cast<int*>(smem + L::off_wf);
+    AccT* s_wv = reinterpret_cast<AccT*>(smem + L::off_wv);
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int m = A.rows;
+    const int rows_c = A.rows_c;
     const unsigned last_col = static_cast<unsigned>(A.cols - 1);
 
     typename Epi::State est;
@@ -125,10 +173,12 @@ __global__ void __launch_bounds__(BLOCK)
         const int t = first + i * stride;
         const int s = i % STAGES;
         const size_t off = size_t(t) * T;
-        mbar_arrive_expect_tx(&s_bar[s], unsigned(T) * 4u * L::kArrays);
+        mbar_arrive_expect_tx(&s_bar[s], L::tx_bytes);
         tma_bulk_g2s(s_col + s * T, A.col + off, T * 4, &s_bar[s], policy);
         tma_bulk_g2s(s_val + s * T, A.val + off, T * 4, &s_bar[s], policy);
         if constexpr (kLo) tma_bulk_g2s(s_lo + s * T, A.val_lo + off, T * 4, &s_bar[s], policy);
+        tma_bulk_g2s(s_flags + s * WPT, A.flags + size_t(t) * WPT, unsigned(L::flag_bytes), &s_bar[s], policy);
+        tma_bulk_g2s(s_meta + s, A.meta + t, 16, &s_bar[s], policy);
     };
 
     if (tid == 0) {
@@ -148,32 +198,57 @@ __global__ void __launch_bounds__(BLOCK)
             fence_proxy_async_smem();
             issue(i + STAGES - 1);
         }
-
-        const int r_lo = A.tile_row[t];
-        const int r_hi = A.tile_row[t + 1];
-        const int cnt = r_hi - r_lo + 2;
-        const bool rp_smem = cnt <= L::RP_CAP;
-        if (rp_smem) {
-            for (int j = tid; j < cnt; j += BLOCK) s_rp[j] = A.row_ptr[r_lo + j];
-        }
-        const int* rpb = rp_smem ? (s_rp - r_lo) : A.row_ptr;   // rpb[r] == row_ptr[r]
-
         const bool ok = mbar_wait_bounded(&s_bar[s], parity);
         if (__syncthreads_or(!ok)) {
             failed = true;
             break;
         }
 
-        const int tile_base = t * T;
-        const int tile_end = tile_base + T;
-        const int k0 = tile_base + tid * IPT;
-        const int k1 = k0 + IPT;
+        const int4 meta = s_meta[s];   // first_row, head_t0, tail_span, tail_continues
+        const uint32_t* fl = s_flags + s * WPT;
+        const int q0 = tid * IPT;      // tile-local index of my first entry
 
-        // ---- products: IPT independent gathers in flight per thread ----
+        // ---- row-start bits of my entries and of the entry after them ----
+        const uint32_t my = (fl[q0 >> 5] >> (q0 & 31)) & kMask;
+        uint32_t next_start;
+        if (tid == BLOCK - 1) next_start = meta.w ? 0u : 1u;
+        else next_start = (fl[(q0 + IPT) >> 5] >> ((q0 + IPT) & 31)) & 1u;
+        const uint32_t ends = (my >> 1) | (next_start << (IPT - 1));   // bit j: entry j ends a row
+
+        // ---- row id of my first entry: first_row + #starts in (0, q0] ----
+        int row0;
+        {
+            // starts in tile entries [0, q0): popcount of the warps before me + lanes before me
+            int before_warp = 0;
+            const int words_before = warp * (32 * IPT / 32);
+            for (int w = lane; w < words_before; w += 32) before_warp += __popc(fl[w]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) before_warp += __shfl_xor_sync(0xffffffffu, before_warp, o);
+            int incl = __popc(my);
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += v;
+            }
+            const int starts_lt_q0 = before_warp + incl - __popc(my);
+            const int s0 = fl[0] & 1u;
+            // #starts in (0, q0] = starts in [0, q0] minus the start at entry 0
+            row0 = meta.x + (starts_lt_q0 + (my & 1u)) - s0;
+        }
+        const bool head_before = (my & 1u) == 0;   // my first row began before my first entry
+
+        // ---- prefetch the epilogue rows I will finish, then gather x ----
+        const int nends = __popc(ends);
+        if (nends > 0 && !kRowMap) {
+            const int r_first = row0;
+            const int r_last = row0 + nends - 1;
+            if (r_first < rows_c) epi.prefetch(r_first);
+            if (r_last != r_first && r_last < rows_c) epi.prefetch(r_last);
+        }
         AccT p[IPT];
         {
-            const int* sc = s_col + s * T + tid * IPT;
-            const float* sv = s_val + s * T + tid * IPT;
+            const int* sc = s_col + s * T + q0;
+            const float* sv = s_val + s * T + q0;
 #pragma unroll
             for (int j = 0; j < IPT; j += 4) {
                 const int4 c4 = *reinterpret_cast<const int4*>(sc + j);
@@ -182,13 +257,13 @@ __global__ void __launch_bounds__(BLOCK)
                 const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
                 float ll[4] = {0.f, 0.f, 0.f, 0.f};
                 if constexpr (kLo) {
-                    const float4 l4 = *reinterpret_cast<const float4*>(s_lo + s * T + tid * IPT + j);
+                    const float4 l4 = *reinterpret_cast<const float4*>(s_lo + s * T + q0 + j);
                     ll[0] = l4.x; ll[1] = l4.y; ll[2] = l4.z; ll[3] = l4.w;
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     unsigned ci = static_cast<unsigned>(cc[q]);
-                    ci = ci < last_col ? ci : last_col;   // cheap guard: never gather out of bounds
+                    ci = ci < last_col ? ci : last_col;   // never gather out of bounds
                     const XT xv = __ldg(x + ci);
                     if constexpr (kLo) {
                         p[j + q] = (static_cast<AccT>(vv[q]) + static_cast<AccT>(ll[q])) *
@@ -200,91 +275,91 @@ __global__ void __launch_bounds__(BLOCK)
             }
         }
 
-        // ---- first row whose end lies beyond k0 ----
-        int r;
-        {
-            int lo = r_lo, hi = r_hi;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (rpb[mid + 1] > k0) hi = mid; else lo = mid + 1;
-            }
-            r = (t == 0 && tid == 0) ? 0 : lo;
-        }
+        auto emit = [&](int row_c, AccT v) {
+            if (row_c >= rows_c) return;   // virtual padding row
+            const int r = kRowMap ? A.row_map[row_c] : row_c;
+            epi.apply(est, r, v);
+        };
 
-        // ---- walk items and row boundaries ----
+        // ---- walk my entries; finish the rows that end here ----
         AccT acc = AccT(0);
+        int cur = row0;
         int nemit = 0;
-        int head_row = -1;
         AccT head_acc = AccT(0);
+        bool head_pending = false;
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
-            const int k = k0 + j;
-            while (r < m && rpb[r + 1] <= k) {
-                if (nemit == 0 && rpb[r] < k0) { head_row = r; head_acc = acc; }
-                else epi.apply(est, r, acc);
-                ++nemit; acc = AccT(0); ++r;
-            }
             acc += p[j];
-        }
-        while (r < m && rpb[r + 1] <= k1) {
-            if (nemit == 0 && rpb[r] < k0) { head_row = r; head_acc = acc; }
-            else epi.apply(est, r, acc);
-            ++nemit; acc = AccT(0); ++r;
+            if ((ends >> j) & 1u) {
+                if (nemit == 0 && head_before) { head_acc = acc; head_pending = true; }
+                else emit(cur, acc);
+                ++nemit;
+                ++cur;
+                acc = AccT(0);
+            }
         }
 
-        // ---- segmented block scan of (tail row, tail partial) ----
-        int krow = r;
-        AccT kval = acc;
+        // ---- segmented block scan of (row end seen, open partial) ----
+        SegPair<AccT> a{nemit > 0 ? 1 : 0, acc};
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const int ro = __shfl_up_sync(0xffffffffu, krow, d);
-            const AccT vo = __shfl_up_sync(0xffffffffu, kval, d);
-            if (lane >= d && ro == krow) kval += vo;
+            const int fo = __shfl_up_sync(0xffffffffu, a.f, d);
+            const AccT vo = __shfl_up_sync(0xffffffffu, a.v, d);
+            if (lane >= d) { if (!a.f) a.v += vo; a.f |= fo; }
         }
-        if (lane == 31) { s_wrow[warp] = krow; s_wval[warp] = kval; }
+        if (lane == 31) { s_wf[warp] = a.f; s_wv[warp] = a.v; }
         __syncthreads();
-        int prow = -1;
-        AccT pval = AccT(0);
+        SegPair<AccT> pre{0, AccT(0)};
 #pragma unroll
         for (int w = 0; w < NW; ++w) {
             if (w < warp) {
-                const int rw = s_wrow[w];
-                const AccT vw = s_wval[w];
-                if (rw == prow) pval += vw; else { prow = rw; pval = vw; }
+                const int fw = s_wf[w];
+                const AccT vw = s_wv[w];
+                if (fw) { pre.f = 1; pre.v = vw; } else { pre.v += vw; }
             }
         }
-        if (krow == prow) kval += pval;   // block-inclusive value of this thread
-        int erow = __shfl_up_sync(0xffffffffu, krow, 1);
-        AccT eval = __shfl_up_sync(0xffffffffu, kval, 1);
-        if (lane == 0) { erow = prow; eval = pval; }
+        SegPair<AccT> ex;   // exclusive: partial of the row open at my first entry
+        {
+            const int fo = __shfl_up_sync(0xffffffffu, a.f, 1);
+            const AccT vo = __shfl_up_sync(0xffffffffu, a.v, 1);
+            if (lane == 0) ex = pre;
+            else { ex.f = pre.f | fo; ex.v = fo ? vo : pre.v + vo; }
+        }
+        const AccT carry_in = ex.v;
 
-        auto cross_tile = [&](int row, AccT v, bool is_tail) {
+        auto arrive = [&](int row_c, AccT v, bool is_tail, int slot, int count) {
             carry[2 * t + (is_tail ? 1 : 0)] = v;
-            __threadfence();
-            const int t0 = rpb[row] / T;
-            const int t1 = (rpb[row + 1] - 1) / T;
-            const int old = atomicAdd(&A.counter[t0], 1);
-            if (old == t1 - t0) {
-                __threadfence();
-                AccT sum = ld_cg(&carry[2 * t0 + 1]);
-                for (int tt = t0 + 1; tt <= t1; ++tt) sum += ld_cg(&carry[2 * tt]);
-                A.counter[t0] = 0;
-                epi.apply(est, row, sum);
+            const int old = atomic_add_acq_rel_gpu(&A.counter[slot], 1);
+            if (old == count - 1) {
+                AccT sum = ld_relaxed_gpu(&carry[2 * slot + 1]);
+                for (int tt = slot + 1; tt < slot + count; ++tt) sum += ld_relaxed_gpu(&carry[2 * tt]);
+                A.counter[slot] = 0;
+                emit(row_c, sum);
             }
         };
 
-        if (head_row >= 0) {
-            const AccT tot = head_acc + (erow == head_row ? eval : AccT(0));
-            if (rpb[head_row] >= tile_base) epi.apply(est, head_row, tot);
-            else cross_tile(head_row, tot, false);
+        // first row finished by this thread began before my first entry
+        if (head_pending) {
+            const AccT tot = head_acc + carry_in;
+            if (row0 == meta.x && meta.y >= 0) {
+                // it began in an earlier tile: this tile holds its last piece
+                const int slot = meta.y;
+                arrive(row0, tot, false, slot, A.meta[slot].z);
+            } else {
+                emit(row0, tot);
+            }
         }
-        // The tile's last row continues into the next tile: a piece of it
-        // lies in this tile only when the row starts before tile_end (a row
-        // starting exactly on the boundary belongs wholly to later tiles).
-        if (tid == BLOCK - 1 && krow < m && rpb[krow] < tile_end && rpb[krow + 1] > tile_end) {
-            cross_tile(krow, kval, rpb[krow] >= tile_base);
+        // the tile's last row continues into the next tile
+        if (tid == BLOCK - 1 && meta.w) {
+            const AccT tot = nemit > 0 ? acc : carry_in + acc;
+            if (cur == meta.x && meta.y >= 0) {
+                const int slot = meta.y;   // a middle piece of a row begun earlier
+                arrive(cur, tot, false, slot, A.meta[slot].z);
+            } else {
+                arrive(cur, tot, true, t, meta.z);   // the row begins in this tile
+            }
         }
-        __syncthreads();   // stage s, s_rp and s_w* free for reuse
+        __syncthreads();   // stage s and the scan scratch are free for reuse
     }
 
     if (failed) {
@@ -299,18 +374,19 @@ __global__ void __launch_bounds__(BLOCK)
     epi.finish(est);
 }
 
-// Rows of an operand without any non-zero (nnz == 0): every row sees 0.
+// Rows without entries see the value 0 (empty-row list, or every row when nnz == 0).
 template <class Epi, typename AccT>
-__global__ void __launch_bounds__(256) zero_rows_kernel(int rows, const Epi epi) {
+__global__ void __launch_bounds__(256)
+    empty_rows_kernel(int count, const int* __restrict__ list, const Epi epi) {
     typename Epi::State est;
     epi.init(est);
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
-        epi.apply(est, r, AccT(0));
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
+        epi.apply(est, list ? list[k] : k, AccT(0));
     epi.finish(est);
 }
 
 // ---------------------------------------------------------------------------
-// Block-level reduction helper used by epilogues' finish().
+// Block-level reduction helpers used by epilogues' finish().
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
