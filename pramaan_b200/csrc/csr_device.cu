@@ -111,25 +111,37 @@ __device__ int row_of_entry(const int* __restrict__ rp_c, int rows_c, long long 
     return lo;
 }
 
-// meta[t] = {first_row, head_t0, tail_span, tail_continues}
+// meta[t] = {first_row, tail_continues, 0, 0}
 //   first_row      compacted row holding the tile's first entry
-//   head_t0        tile where that row begins, or -1 when it begins at this tile
 //   tail_continues 1 when the row holding the tile's last entry continues into
 //                  the next tile
-//   tail_span      when that row also begins in this tile: the number of tiles
-//                  it touches (the arrivals its counter waits for), else 0
+// begins[t] = 1 when that continuing row also begins in tile t: such a row is
+// a crossing row, listed once, at the tile where it begins.
 __global__ void meta_kernel(const int* __restrict__ rp_c, int rows_c, int tiles, int T,
-                            int4* __restrict__ meta) {
+                            int4* __restrict__ meta, int* __restrict__ begins) {
     PB_GRID_STRIDE(t, tiles) {
         const long long base = t * (long long)T, last = base + T - 1;
         const int fr = row_of_entry(rp_c, rows_c, base);
-        const int fstart = rp_c[fr];
-        const int head_t0 = fstart < base ? int(fstart / T) : -1;
         const int tr = row_of_entry(rp_c, rows_c, last);
         const long long tend = rp_c[tr + 1];
         const int cont = (tr < rows_c && tend > last + 1) ? 1 : 0;
-        const int span = (cont && rp_c[tr] >= base) ? int((tend - 1) / T - t + 1) : 0;
-        meta[t] = make_int4(fr, head_t0, span, cont);
+        meta[t] = make_int4(fr, cont, 0, 0);
+        begins[t] = (cont && rp_c[tr] >= base) ? 1 : 0;
+    }
+}
+
+// cross[idx[t]] = {original row, t, tiles touched} for every tile where a
+// crossing row begins.
+__global__ void cross_kernel(const int* __restrict__ rp_c, const int* __restrict__ row_map,
+                             int rows_c, int tiles, int T, const int* __restrict__ begins,
+                             const int* __restrict__ idx, int4* __restrict__ cross) {
+    PB_GRID_STRIDE(t, tiles) {
+        if (!begins[t]) continue;
+        const long long last = t * (long long)T + T - 1;
+        const int tr = row_of_entry(rp_c, rows_c, last);
+        const long long tend = rp_c[tr + 1];
+        const int span = int((tend - 1) / T - t + 1);
+        cross[idx[t]] = make_int4(row_map ? row_map[tr] : tr, int(t), span, 0);
     }
 }
 
@@ -229,26 +241,39 @@ void CsrDevice::finalize(cudaStream_t st) {
     rp_tail_kernel<<<1, 1, 0, st>>>(rp_c.get(), rows_c, nnz, nnz_pad);
     PB_CUDA_CHECK(cudaGetLastError());
 
-    // ---- row-start bitmap and tile descriptors ----
+    // ---- row-start bitmap, tile descriptors, crossing rows ----
     flags.alloc(size_t(nnz_pad / 32 > 0 ? nnz_pad / 32 : 1));
     meta.alloc(size_t(num_tiles > 0 ? num_tiles : 1));
     PB_CUDA_CHECK(cudaMemsetAsync(flags.get(), 0, flags.bytes(), st));
+    num_cross = 0;
+    cross.reset();
     if (num_tiles > 0) {
         flags_kernel<<<grid_1d((long long)rows_c + 1), kThreads, 0, st>>>(rp_c.get(), rows_c, nnz,
                                                                          nnz_pad, flags.get());
+        DevBuf<int> begins(static_cast<size_t>(num_tiles)), bidx(static_cast<size_t>(num_tiles));
         meta_kernel<<<grid_1d(num_tiles), kThreads, 0, st>>>(rp_c.get(), rows_c, num_tiles, kSpmvTile,
-                                                             meta.get());
+                                                             meta.get(), begins.get());
         PB_CUDA_CHECK(cudaGetLastError());
+        size_t tb = 0;
+        PB_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tb, begins.get(), bidx.get(), num_tiles, st));
+        DevBuf<unsigned char> temp(tb > 0 ? tb : 1);
+        PB_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(temp.get(), tb, begins.get(), bidx.get(), num_tiles, st));
+        int last_idx = 0, last_b = 0;
+        PB_CUDA_CHECK(cudaMemcpyAsync(&last_idx, bidx.get() + num_tiles - 1, 4, cudaMemcpyDeviceToHost, st));
+        PB_CUDA_CHECK(cudaMemcpyAsync(&last_b, begins.get() + num_tiles - 1, 4, cudaMemcpyDeviceToHost, st));
+        PB_CUDA_CHECK(cudaStreamSynchronize(st));
+        num_cross = last_idx + last_b;
+        if (num_cross > 0) {
+            cross.alloc(static_cast<size_t>(num_cross));
+            cross_kernel<<<grid_1d(num_tiles), kThreads, 0, st>>>(
+                rp_c.get(), num_empty > 0 ? row_map.get() : nullptr, rows_c, num_tiles, kSpmvTile,
+                begins.get(), bidx.get(), cross.get());
+            PB_CUDA_CHECK(cudaGetLastError());
+        }
     }
-    counter.alloc(size_t(num_tiles > 0 ? num_tiles : 1));
     carry.alloc(size_t(2) * (num_tiles > 0 ? num_tiles : 1));
-    reset_counters(st);
     PB_CUDA_CHECK(cudaMemsetAsync(carry.get(), 0, carry.bytes(), st));
     PB_CUDA_CHECK(cudaStreamSynchronize(st));   // temporaries are freed on return
-}
-
-void CsrDevice::reset_counters(cudaStream_t st) {
-    if (counter.get()) PB_CUDA_CHECK(cudaMemsetAsync(counter.get(), 0, counter.bytes(), st));
 }
 
 static void upload_structure(CsrDevice& A, int rows, int cols, int nnz, const int* h_row_ptr,

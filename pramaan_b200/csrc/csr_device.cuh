@@ -8,13 +8,13 @@
 //   val_lo     fp32  [nnz_pad]         FP32(value - val), kept only when some
 //                                      value is not exactly representable
 //   flags      u32   [nnz_pad / 32]    bit q: entry q starts a non-empty row
-//   meta       int4  [tiles]           {first_row, head_t0, tail_span, tail_continues}
+//   meta       int4  [tiles]           {first_row, tail_continues, 0, 0}
 //   row_map    int32 [rows_c]          original row of each non-empty row (only
 //                                      when empty rows exist)
 //   empty_rows int32 [rows - rows_c]   rows without entries
-//   carry      f64   [2 * tiles]       cross-tile partials (scratch)
-//   counter    int32 [tiles]           cross-tile arrival counters (scratch, zero at rest)
-// nnz_pad is a multiple of the tile (2048 entries), and every array starts on
+//   cross      int4  [crossing rows]   {row, first tile, tiles, 0} per row spanning tiles
+//   carry      f64   [2 * tiles]       per-tile partials of crossing rows (scratch)
+// nnz_pad is a multiple of the tile (256 entries), and every array starts on
 // a 256-byte boundary (cudaMalloc), so each tile's slabs are 16-byte aligned
 // for the bulk copies.
 #pragma once
@@ -67,23 +67,23 @@ private:
 class CsrDevice {
 public:
     int rows = 0, cols = 0, nnz = 0, nnz_pad = 0, num_tiles = 0;
-    int rows_c = 0, num_empty = 0;
+    int rows_c = 0, num_empty = 0, num_cross = 0;
     bool has_lo = false;
-    DevBuf<int> row_ptr, col, row_map, empty_rows, counter;
+    DevBuf<int> row_ptr, col, row_map, empty_rows;
     DevBuf<float> val, val_lo;
     DevBuf<uint32_t> flags;
-    DevBuf<int4> meta;
+    DevBuf<int4> meta, cross;
     DevBuf<double> carry;
 
     CsrView view(bool with_lo) const {
         CsrView v;
         v.rows = rows; v.cols = cols; v.nnz = nnz; v.nnz_pad = nnz_pad; v.num_tiles = num_tiles;
-        v.rows_c = rows_c; v.num_empty = num_empty;
+        v.rows_c = rows_c; v.num_empty = num_empty; v.num_cross = num_cross;
         v.col = col.get(); v.val = val.get();
         v.val_lo = (with_lo && has_lo) ? val_lo.get() : nullptr;
         v.flags = flags.get(); v.meta = meta.get();
         v.row_map = row_map.get(); v.empty_rows = empty_rows.get();
-        v.carry = carry.get(); v.counter = counter.get();
+        v.cross = cross.get(); v.carry = carry.get();
         return v;
     }
 
@@ -96,13 +96,11 @@ public:
 
     // Allocates the padded arrays for the given shape.
     void allocate(int rows_, int cols_, int nnz_, bool lo);
-    // Builds flags / meta / row compaction from row_ptr and zeroes the scratch.
+    // Builds flags / meta / row compaction / crossing rows from row_ptr.
     void finalize(cudaStream_t st);
-    // Zeroes the cross-tile counters (after an aborted launch).
-    void reset_counters(cudaStream_t st);
     size_t device_bytes() const {
         return row_ptr.bytes() + col.bytes() + row_map.bytes() + empty_rows.bytes() +
-               counter.bytes() + val.bytes() + val_lo.bytes() + flags.bytes() + meta.bytes() +
+               val.bytes() + val_lo.bytes() + flags.bytes() + meta.bytes() + cross.bytes() +
                carry.bytes();
     }
 };
@@ -125,12 +123,15 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st);
 // ---------------------------------------------------------------------------
 int device_sm_count(int dev);
 
+constexpr int kSpmvWarps = 8;     // warps per block (each with its own ring)
+constexpr int kSpmvStages = 4;    // ring depth per warp
+
 template <class Epi, typename AccT, typename XT, bool kLo>
 struct SpmvLauncher {
-    using L = SpmvSmemLayout<kSpmvBlock, kSpmvIpt, kSpmvStages, kLo, AccT>;
+    using L = SpmvSmemLayout<kSpmvWarps, kSpmvStages, kLo, AccT>;
     template <bool kRowMap>
     static constexpr auto kernel() {
-        return &spmv_tile_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvBlock, kSpmvIpt, kSpmvStages>;
+        return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvWarps, kSpmvStages>;
     }
     template <bool kRowMap>
     static int blocks_per_sm_impl(int dev) {
@@ -141,8 +142,8 @@ struct SpmvLauncher {
         PB_CUDA_CHECK(cudaFuncSetAttribute(kernel<kRowMap>(),
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes)));
         int nb = 0;
-        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel<kRowMap>(), kSpmvBlock,
-                                                                    L::bytes));
+        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel<kRowMap>(),
+                                                                    kSpmvWarps * 32, L::bytes));
         if (nb < 1) nb = 1;
         cache[dev].store(nb, std::memory_order_relaxed);
         return nb;
@@ -161,25 +162,28 @@ struct SpmvLauncher {
             const long long cap = (long long)(mapped ? blocks_per_sm_impl<true>(dev)
                                                      : blocks_per_sm_impl<false>(dev)) *
                                   device_sm_count(dev);
-            const int grid = int(A.num_tiles < cap ? A.num_tiles : cap);
+            const long long need = (A.num_tiles + kSpmvWarps - 1) / kSpmvWarps;
+            const int grid = int(need < cap ? need : cap);
             if (mapped) {
                 auto k = kernel<true>();
-                k<<<grid, kSpmvBlock, L::bytes, st>>>(A, x, epi, dev_status);
+                k<<<grid, kSpmvWarps * 32, L::bytes, st>>>(A, x, epi, dev_status);
             } else {
                 auto k = kernel<false>();
-                k<<<grid, kSpmvBlock, L::bytes, st>>>(A, x, epi, dev_status);
+                k<<<grid, kSpmvWarps * 32, L::bytes, st>>>(A, x, epi, dev_status);
             }
             PB_CUDA_CHECK(cudaGetLastError());
         }
-        if (A.num_empty > 0) {
-            const int grid = (A.num_empty + 255) / 256 < 4096 ? (A.num_empty + 255) / 256 : 4096;
-            empty_rows_kernel<Epi, AccT><<<grid, 256, 0, st>>>(A.num_empty, A.empty_rows, epi);
+        const int fix = A.num_cross + A.num_empty;
+        if (fix > 0) {
+            const int grid = (fix + 255) / 256 < 2048 ? (fix + 255) / 256 : 2048;
+            spmv_fixup_kernel<Epi, AccT><<<grid, 256, 0, st>>>(A, epi);
             PB_CUDA_CHECK(cudaGetLastError());
         }
     }
-    // Kernels launched by one launch() call.
+    // Kernels one launch() call issues.
     static int launches(const CsrView& A) {
-        return (A.rows > 0 && A.num_tiles > 0 ? 1 : 0) + (A.rows > 0 && A.num_empty > 0 ? 1 : 0);
+        if (A.rows <= 0) return 0;
+        return (A.num_tiles > 0 ? 1 : 0) + (A.num_cross + A.num_empty > 0 ? 1 : 0);
     }
 };
 

@@ -306,8 +306,6 @@ void PdhgEngine::check_device_status() {
     PB_CUDA_CHECK(cudaStreamSynchronize(st_));
     if (*h_status_ & kDevErrTimeout) {
         PB_CUDA_CHECK(cudaMemsetAsync(status_.get(), 0, sizeof(int), st_));
-        A_.reset_counters(st_);
-        AT_.reset_counters(st_);
         PB_CUDA_CHECK(cudaStreamSynchronize(st_));
         throw DeviceTimeout("device wait on a bulk copy exceeded its time limit; iterate discarded");
     }

@@ -7,40 +7,45 @@
 // both products are gathers and both are deterministic run to run.
 //
 // Tiled operand format (built once per matrix, see csr_device.cu)
-//   The non-zeros are cut into tiles of T = BLOCK*IPT consecutive entries.
-//   Per tile, four slabs sit at 16-byte aligned offsets:
-//     col   int32[T]      column indices
-//     val   fp32 [T]      values (FP32-rounded)      [+ val_lo fp32[T]]
-//     flags u32 [T/32]    bit q set <=> entry q starts a row
-//     meta  int4          {first_row, head_t0, tail_span, tail_continues}
+//   The non-zeros are cut into tiles of TW = 32*IPT consecutive entries, one
+//   tile per warp at a time.  Per tile, four slabs sit at 16-byte aligned
+//   offsets:
+//     col   int32[TW]     column indices
+//     val   fp32 [TW]     values (FP32-rounded)      [+ val_lo fp32[TW]]
+//     flags u32 [TW/32]   bit q set <=> entry q starts a row
+//     meta  int4          {first_row, tail_continues, 0, 0}
 //   Empty rows are compacted out (an optional row_map gives the original row
-//   of every compacted row; empty rows get their epilogue from a separate
-//   pass), and the padding after the last entry forms a virtual row that is
-//   never emitted.  Row ids therefore follow from the bitmap alone:
-//   row(q) = first_row + #starts in (0, q], and the kernel never reads
+//   of every compacted row) and the padding after the last entry forms a
+//   virtual row that is never emitted, so row ids follow from the bitmap
+//   alone: row(q) = first_row + #starts in (0, q].  The kernel never reads
 //   row_ptr.
 //
-// Schedule
-//   A persistent grid (a multiple of the SM count) walks the tiles with a
-//   static stride.  Thread 0 streams every tile's four slabs into a
-//   STAGES-deep shared-memory ring with 1-D TMA bulk copies
-//   (cp.async.bulk ... mbarrier::complete_tx, L2 evict_first) while the
-//   block works on earlier tiles; waits on the ring's mbarriers are bounded.
-//   Every thread owns IPT consecutive entries.  Row ids come from popcounts
-//   of the bitmap (warp shuffles, no block barrier), the epilogue's vectors
-//   for the rows a thread will finish are prefetched into L2 together with
-//   the x gathers, and one segmented block scan (shuffles + one barrier)
-//   carries open-row partial sums across threads.  A row that crosses tile
-//   boundaries is finished by the "last arriver": each tile holding a piece
-//   stores its partial in carry[], bumps the row's counter with an acq_rel
-//   atomic, and the tile that completes the count adds the pieces in tile
-//   order.  No block ever waits on another block, and every sum has a fixed
-//   order, so results are bit-identical between runs.
+// Schedule (spmv_warp_kernel)
+//   A persistent grid walks the tiles; every warp owns a private STAGES-deep
+//   shared-memory ring that its lane 0 fills with 1-D TMA bulk copies
+//   (cp.async.bulk ... mbarrier::complete_tx, L2 evict_first), so warps never
+//   wait on each other: there is no block barrier in the main loop.  Each
+//   lane owns IPT consecutive entries: row ids come from popcounts of the
+//   bitmap (shuffles), the epilogue's vectors for the rows the lane will
+//   finish are prefetched into L2 together with the x gathers, and a
+//   segmented warp scan carries open-row partial sums across lanes.  Rows
+//   that end inside the tile get their epilogue on the spot.  A row that
+//   crosses tiles leaves one partial per tile in carry[] (head piece: the
+//   tile holds its end or a middle part; tail piece: it begins in the tile).
+//
+// Completion (spmv_fixup_kernel, launched right after on the same stream)
+//   For every crossing row the fixup adds its pieces in tile order and runs
+//   the epilogue; it also gives every empty row the value 0.  All sums have a
+//   fixed order, so results are bit-identical between runs, and no thread
+//   ever waits on another block.
 #pragma once
 
 #include "common.cuh"
 
 namespace pb {
+
+constexpr int kSpmvIpt = 8;                  // entries per lane
+constexpr int kSpmvTile = 32 * kSpmvIpt;     // entries per warp-tile (format unit)
 
 // Device view of one CSR operand in the tiled format.
 struct CsrView {
@@ -49,41 +54,35 @@ struct CsrView {
     int nnz = 0, nnz_pad = 0, num_tiles = 0;
     int rows_c = 0;        // non-empty (compacted) rows
     int num_empty = 0;     // rows without entries
-    const int* col = nullptr;        // nnz_pad
-    const float* val = nullptr;      // nnz_pad
-    const float* val_lo = nullptr;   // nnz_pad or null
-    const uint32_t* flags = nullptr; // nnz_pad / 32
-    const int4* meta = nullptr;      // num_tiles
-    const int* row_map = nullptr;    // rows_c (null: identity)
-    const int* empty_rows = nullptr; // num_empty
-    void* carry = nullptr;           // 2 * num_tiles accumulators (8-byte slots)
-    int* counter = nullptr;          // num_tiles, zero between launches
+    int num_cross = 0;     // rows spanning more than one tile
+    const int* col = nullptr;         // nnz_pad
+    const float* val = nullptr;       // nnz_pad
+    const float* val_lo = nullptr;    // nnz_pad or null
+    const uint32_t* flags = nullptr;  // nnz_pad / 32
+    const int4* meta = nullptr;       // num_tiles: {first_row, tail_continues, 0, 0}
+    const int* row_map = nullptr;     // rows_c (null: identity)
+    const int* empty_rows = nullptr;  // num_empty
+    const int4* cross = nullptr;      // num_cross: {original row, first tile, tiles, 0}
+    void* carry = nullptr;            // 2 * num_tiles accumulators (8-byte slots)
 };
 
-constexpr int kSpmvBlock = 256;
-constexpr int kSpmvIpt = 8;
-constexpr int kSpmvTile = kSpmvBlock * kSpmvIpt;
-constexpr int kSpmvStages = 4;
-
-template <int BLOCK, int IPT, int STAGES, bool kLo, typename AccT>
+template <int WARPS, int STAGES, bool kLo, typename AccT>
 struct SpmvSmemLayout {
-    static constexpr int T = BLOCK * IPT;
-    static constexpr int NW = BLOCK / 32;
+    static constexpr int TW = kSpmvTile;
+    static constexpr int FW = TW / 32;
     static constexpr int kArrays = kLo ? 3 : 2;
-    static constexpr size_t flag_bytes = size_t(T) / 8;
-    static constexpr size_t stage_bytes = size_t(T) * 4 * kArrays + flag_bytes + 16;
-    static constexpr size_t off_col = 0;
-    static constexpr size_t off_val = off_col + size_t(STAGES) * T * 4;
-    static constexpr size_t off_lo = off_val + size_t(STAGES) * T * 4;
-    static constexpr size_t off_flags = off_val + size_t(STAGES) * T * 4 * (kArrays - 1);
-    static constexpr size_t off_meta = off_flags + size_t(STAGES) * flag_bytes;
-    static constexpr size_t off_bar = off_meta + size_t(STAGES) * 16;
-    static constexpr size_t off_wf = off_bar + size_t(STAGES) * 8;
-    static constexpr size_t off_wv = off_wf + 8 * ((size_t(NW) * 4 + 7) / 8);
-    static constexpr size_t bytes = ((off_wv + size_t(NW) * sizeof(AccT)) + 127) / 128 * 128;
+    static constexpr size_t slab = size_t(TW) * 4;
+    static constexpr size_t off_val = slab;
+    static constexpr size_t off_lo = 2 * slab;
+    static constexpr size_t off_flags = slab * kArrays;
+    static constexpr size_t off_meta = off_flags + size_t(FW) * 4;
+    static constexpr size_t stage_bytes = off_meta + 16;
+    static constexpr size_t warp_bytes = size_t(STAGES) * stage_bytes;
+    static constexpr size_t off_bar = size_t(WARPS) * warp_bytes;
+    static constexpr size_t bytes = ((off_bar + size_t(WARPS) * STAGES * 8) + 127) / 128 * 128;
     static constexpr unsigned tx_bytes = unsigned(stage_bytes);
-    static_assert(T % 32 == 0 && 32 % IPT == 0, "IPT must divide 32");
-    static_assert((size_t(T) * 4) % 16 == 0 && flag_bytes % 16 == 0, "TMA slabs must be 16-byte multiples");
+    static_assert(stage_bytes % 16 == 0 && (size_t(FW) * 4) % 16 == 0,
+                  "TMA slabs must be 16-byte multiples");
 };
 
 // Epilogue concept:
@@ -95,60 +94,26 @@ struct SpmvSmemLayout {
 //     __device__ void finish(State&) const;                // once by every thread at exit
 //   };
 
-__device__ __forceinline__ int atomic_add_acq_rel_gpu(int* p, int v) {
-    int old;
-    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-template <typename T>
-__device__ __forceinline__ T ld_relaxed_gpu(const T* p);
-template <>
-__device__ __forceinline__ float ld_relaxed_gpu<float>(const float* p) {
-    float v;
-    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
-    return v;
-}
-template <>
-__device__ __forceinline__ double ld_relaxed_gpu<double>(const double* p) {
-    double v;
-    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-    return v;
-}
-
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-template <typename AccT>
-struct SegPair {   // (row end seen, open-row partial)
-    int f;
-    AccT v;
-};
-
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int BLOCK, int IPT, int STAGES>
-__global__ void __launch_bounds__(BLOCK)
-    spmv_tile_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES>
+__global__ void __launch_bounds__(WARPS * 32)
+    spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
                      int* __restrict__ dev_status) {
-    using L = SpmvSmemLayout<BLOCK, IPT, STAGES, kLo, AccT>;
-    constexpr int T = L::T;
-    constexpr int NW = L::NW;
-    constexpr int WPT = T / 32;              // flag words per tile
+    using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT>;
+    constexpr int IPT = kSpmvIpt;
+    constexpr int TW = L::TW;
+    constexpr int FW = L::FW;
     constexpr unsigned kMask = (IPT == 32) ? 0xffffffffu : ((1u << IPT) - 1u);
 
     extern __shared__ __align__(128) unsigned char smem[];
-    int* s_col = reinterpret_cast<int*>(smem + L::off_col);
-    float* s_val = reinterpret_cast<float*>(smem + L::off_val);
-    float* s_lo = reinterpret_cast<float*>(smem + L::off_lo);
-    uint32_t* s_flags = reinterpret_cast<uint32_t*>(smem + L::off_flags);
-    int4* s_meta = reinterpret_cast<int4*>(smem + L::off_meta);
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem + L::off_bar);
-    int* s_wf = reinterpret_cast<int*>(smem + L::off_wf);
-    AccT* s_wv = reinterpret_cast<AccT*>(smem + L::off_wv);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    unsigned char* ring = smem + size_t(warp) * L::warp_bytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::off_bar) + warp * STAGES;
 
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
     const int rows_c = A.rows_c;
     const unsigned last_col = static_cast<unsigned>(A.cols - 1);
 
@@ -156,34 +121,34 @@ __global__ void __launch_bounds__(BLOCK)
     epi.init(est);
 
     const int nt = A.num_tiles;
-    const int first = blockIdx.x;
-    const int stride = gridDim.x;
-    const int mine = first < nt ? (nt - first + stride - 1) / stride : 0;
-
-    if (tid == 0) {
-        for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
+    const int gw = blockIdx.x * WARPS + warp;
+    const int stride = gridDim.x * WARPS;
+    const int mine = gw < nt ? (nt - gw + stride - 1) / stride : 0;
 
     uint64_t policy = 0;
-    if (tid == 0) policy = l2_policy_evict_first();
+    if (lane == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+        policy = l2_policy_evict_first();
+    }
+    __syncwarp();
 
     auto issue = [&](int i) {
-        const int t = first + i * stride;
+        const int t = gw + i * stride;
         const int s = i % STAGES;
-        const size_t off = size_t(t) * T;
-        mbar_arrive_expect_tx(&s_bar[s], L::tx_bytes);
-        tma_bulk_g2s(s_col + s * T, A.col + off, T * 4, &s_bar[s], policy);
-        tma_bulk_g2s(s_val + s * T, A.val + off, T * 4, &s_bar[s], policy);
-        if constexpr (kLo) tma_bulk_g2s(s_lo + s * T, A.val_lo + off, T * 4, &s_bar[s], policy);
-        tma_bulk_g2s(s_flags + s * WPT, A.flags + size_t(t) * WPT, unsigned(L::flag_bytes), &s_bar[s], policy);
-        tma_bulk_g2s(s_meta + s, A.meta + t, 16, &s_bar[s], policy);
+        unsigned char* st = ring + size_t(s) * L::stage_bytes;
+        const size_t off = size_t(t) * TW;
+        mbar_arrive_expect_tx(&bar[s], L::tx_bytes);
+        tma_bulk_g2s(st, A.col + off, TW * 4, &bar[s], policy);
+        tma_bulk_g2s(st + L::off_val, A.val + off, TW * 4, &bar[s], policy);
+        if constexpr (kLo) tma_bulk_g2s(st + L::off_lo, A.val_lo + off, TW * 4, &bar[s], policy);
+        tma_bulk_g2s(st + L::off_flags, A.flags + size_t(t) * FW, FW * 4, &bar[s], policy);
+        tma_bulk_g2s(st + L::off_meta, A.meta + t, 16, &bar[s], policy);
     };
 
-    if (tid == 0) {
+    if (lane == 0) {
         fence_proxy_async_smem();
-        const int pre = mine < STAGES - 1 ? mine : STAGES - 1;
+        const int pre = mine < STAGES ? mine : STAGES;
         for (int i = 0; i < pre; ++i) issue(i);
     }
 
@@ -191,86 +156,70 @@ __global__ void __launch_bounds__(BLOCK)
     bool failed = false;
     int i = 0;
     for (; i < mine; ++i) {
-        const int t = first + i * stride;
+        const int t = gw + i * stride;
         const int s = i % STAGES;
         const uint32_t parity = (i / STAGES) & 1;
-        if (tid == 0 && i + STAGES - 1 < mine) {
-            fence_proxy_async_smem();
-            issue(i + STAGES - 1);
-        }
-        const bool ok = mbar_wait_bounded(&s_bar[s], parity);
-        if (__syncthreads_or(!ok)) {
+        const bool ok = mbar_wait_bounded(&bar[s], parity);
+        if (__any_sync(0xffffffffu, !ok)) {
             failed = true;
             break;
         }
-
-        const int4 meta = s_meta[s];   // first_row, head_t0, tail_span, tail_continues
-        const uint32_t* fl = s_flags + s * WPT;
-        const int q0 = tid * IPT;      // tile-local index of my first entry
+        const unsigned char* st = ring + size_t(s) * L::stage_bytes;
+        const int* scol = reinterpret_cast<const int*>(st);
+        const float* sval = reinterpret_cast<const float*>(st + L::off_val);
+        const float* slo = reinterpret_cast<const float*>(st + L::off_lo);
+        const uint32_t* fl = reinterpret_cast<const uint32_t*>(st + L::off_flags);
+        const int4 meta = *reinterpret_cast<const int4*>(st + L::off_meta);
+        const int q0 = lane * IPT;   // tile-local index of my first entry
 
         // ---- row-start bits of my entries and of the entry after them ----
         const uint32_t my = (fl[q0 >> 5] >> (q0 & 31)) & kMask;
         uint32_t next_start;
-        if (tid == BLOCK - 1) next_start = meta.w ? 0u : 1u;
+        if (lane == 31) next_start = meta.y ? 0u : 1u;
         else next_start = (fl[(q0 + IPT) >> 5] >> ((q0 + IPT) & 31)) & 1u;
         const uint32_t ends = (my >> 1) | (next_start << (IPT - 1));   // bit j: entry j ends a row
+        const uint32_t s0 = fl[0] & 1u;                                 // tile's first entry starts a row
 
         // ---- row id of my first entry: first_row + #starts in (0, q0] ----
-        int row0;
-        {
-            // starts in tile entries [0, q0): popcount of the warps before me + lanes before me
-            int before_warp = 0;
-            const int words_before = warp * (32 * IPT / 32);
-            for (int w = lane; w < words_before; w += 32) before_warp += __popc(fl[w]);
+        int incl = __popc(my);
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) before_warp += __shfl_xor_sync(0xffffffffu, before_warp, o);
-            int incl = __popc(my);
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d) incl += v;
-            }
-            const int starts_lt_q0 = before_warp + incl - __popc(my);
-            const int s0 = fl[0] & 1u;
-            // #starts in (0, q0] = starts in [0, q0] minus the start at entry 0
-            row0 = meta.x + (starts_lt_q0 + (my & 1u)) - s0;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
         }
+        const int row0 = meta.x + (incl - __popc(my)) + int(my & 1u) - int(s0);
         const bool head_before = (my & 1u) == 0;   // my first row began before my first entry
 
         // ---- prefetch the epilogue rows I will finish, then gather x ----
         const int nends = __popc(ends);
-        if (nends > 0 && !kRowMap) {
-            const int r_first = row0;
-            const int r_last = row0 + nends - 1;
-            if (r_first < rows_c) epi.prefetch(r_first);
-            if (r_last != r_first && r_last < rows_c) epi.prefetch(r_last);
+        if constexpr (!kRowMap) {
+            if (nends > 0) {
+                const int r_last = row0 + nends - 1;
+                if (row0 < rows_c) epi.prefetch(row0);
+                if (r_last != row0 && r_last < rows_c) epi.prefetch(r_last);
+            }
         }
         AccT p[IPT];
-        {
-            const int* sc = s_col + s * T + q0;
-            const float* sv = s_val + s * T + q0;
 #pragma unroll
-            for (int j = 0; j < IPT; j += 4) {
-                const int4 c4 = *reinterpret_cast<const int4*>(sc + j);
-                const float4 v4 = *reinterpret_cast<const float4*>(sv + j);
-                const int cc[4] = {c4.x, c4.y, c4.z, c4.w};
-                const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
-                float ll[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int j = 0; j < IPT; j += 4) {
+            const int4 c4 = *reinterpret_cast<const int4*>(scol + q0 + j);
+            const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
+            const int cc[4] = {c4.x, c4.y, c4.z, c4.w};
+            const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
+            float ll[4] = {0.f, 0.f, 0.f, 0.f};
+            if constexpr (kLo) {
+                const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
+                ll[0] = l4.x; ll[1] = l4.y; ll[2] = l4.z; ll[3] = l4.w;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                unsigned ci = static_cast<unsigned>(cc[q]);
+                ci = ci < last_col ? ci : last_col;   // never gather out of bounds
+                const XT xv = __ldg(x + ci);
                 if constexpr (kLo) {
-                    const float4 l4 = *reinterpret_cast<const float4*>(s_lo + s * T + q0 + j);
-                    ll[0] = l4.x; ll[1] = l4.y; ll[2] = l4.z; ll[3] = l4.w;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    unsigned ci = static_cast<unsigned>(cc[q]);
-                    ci = ci < last_col ? ci : last_col;   // never gather out of bounds
-                    const XT xv = __ldg(x + ci);
-                    if constexpr (kLo) {
-                        p[j + q] = (static_cast<AccT>(vv[q]) + static_cast<AccT>(ll[q])) *
-                                   static_cast<AccT>(xv);
-                    } else {
-                        p[j + q] = static_cast<AccT>(vv[q]) * static_cast<AccT>(xv);
-                    }
+                    p[j + q] = (static_cast<AccT>(vv[q]) + static_cast<AccT>(ll[q])) * static_cast<AccT>(xv);
+                } else {
+                    p[j + q] = static_cast<AccT>(vv[q]) * static_cast<AccT>(xv);
                 }
             }
         }
@@ -299,89 +248,68 @@ __global__ void __launch_bounds__(BLOCK)
             }
         }
 
-        // ---- segmented block scan of (row end seen, open partial) ----
-        SegPair<AccT> a{nemit > 0 ? 1 : 0, acc};
+        // ---- segmented warp scan of (row end seen, open partial) ----
+        int f = nemit > 0 ? 1 : 0;
+        AccT v = acc;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const int fo = __shfl_up_sync(0xffffffffu, a.f, d);
-            const AccT vo = __shfl_up_sync(0xffffffffu, a.v, d);
-            if (lane >= d) { if (!a.f) a.v += vo; a.f |= fo; }
+            const int fo = __shfl_up_sync(0xffffffffu, f, d);
+            const AccT vo = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) { if (!f) v += vo; f |= fo; }
         }
-        if (lane == 31) { s_wf[warp] = a.f; s_wv[warp] = a.v; }
-        __syncthreads();
-        SegPair<AccT> pre{0, AccT(0)};
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            if (w < warp) {
-                const int fw = s_wf[w];
-                const AccT vw = s_wv[w];
-                if (fw) { pre.f = 1; pre.v = vw; } else { pre.v += vw; }
-            }
-        }
-        SegPair<AccT> ex;   // exclusive: partial of the row open at my first entry
-        {
-            const int fo = __shfl_up_sync(0xffffffffu, a.f, 1);
-            const AccT vo = __shfl_up_sync(0xffffffffu, a.v, 1);
-            if (lane == 0) ex = pre;
-            else { ex.f = pre.f | fo; ex.v = fo ? vo : pre.v + vo; }
-        }
-        const AccT carry_in = ex.v;
+        AccT carry_in = __shfl_up_sync(0xffffffffu, v, 1);   // partial of the row open at q0
+        if (lane == 0) carry_in = AccT(0);
 
-        auto arrive = [&](int row_c, AccT v, bool is_tail, int slot, int count) {
-            carry[2 * t + (is_tail ? 1 : 0)] = v;
-            const int old = atomic_add_acq_rel_gpu(&A.counter[slot], 1);
-            if (old == count - 1) {
-                AccT sum = ld_relaxed_gpu(&carry[2 * slot + 1]);
-                for (int tt = slot + 1; tt < slot + count; ++tt) sum += ld_relaxed_gpu(&carry[2 * tt]);
-                A.counter[slot] = 0;
-                emit(row_c, sum);
-            }
-        };
-
-        // first row finished by this thread began before my first entry
+        const bool first_began_before = s0 == 0;   // tile's first row began in an earlier tile
         if (head_pending) {
             const AccT tot = head_acc + carry_in;
-            if (row0 == meta.x && meta.y >= 0) {
-                // it began in an earlier tile: this tile holds its last piece
-                const int slot = meta.y;
-                arrive(row0, tot, false, slot, A.meta[slot].z);
-            } else {
-                emit(row0, tot);
-            }
+            if (row0 == meta.x && first_began_before) carry[2 * t] = tot;   // last piece of a crossing row
+            else emit(row0, tot);
         }
-        // the tile's last row continues into the next tile
-        if (tid == BLOCK - 1 && meta.w) {
+        if (lane == 31 && meta.y) {   // the tile's last row continues into the next tile
             const AccT tot = nemit > 0 ? acc : carry_in + acc;
-            if (cur == meta.x && meta.y >= 0) {
-                const int slot = meta.y;   // a middle piece of a row begun earlier
-                arrive(cur, tot, false, slot, A.meta[slot].z);
-            } else {
-                arrive(cur, tot, true, t, meta.z);   // the row begins in this tile
-            }
+            if (cur == meta.x && first_began_before) carry[2 * t] = tot;    // middle piece
+            else carry[2 * t + 1] = tot;                                    // first piece
         }
-        __syncthreads();   // stage s and the scan scratch are free for reuse
+
+        __syncwarp();   // every lane is done with stage s
+        if (lane == 0 && i + STAGES < mine) {
+            fence_proxy_async_smem();
+            issue(i + STAGES);
+        }
     }
 
     if (failed) {
-        if (tid == 0) {
+        if (lane == 0) {
             atomicOr(dev_status, kDevErrTimeout);
-            // Let every bulk copy this block issued land before the block retires.
+            // Let every bulk copy this warp issued land before it retires.
             const int hi = (i + STAGES) < mine ? (i + STAGES) : mine;
-            for (int j = i; j < hi; ++j) (void)mbar_wait_bounded(&s_bar[j % STAGES], (j / STAGES) & 1);
+            for (int j = i; j < hi; ++j) (void)mbar_wait_bounded(&bar[j % STAGES], (j / STAGES) & 1);
         }
-        __syncthreads();
+        __syncwarp();
     }
     epi.finish(est);
 }
 
-// Rows without entries see the value 0 (empty-row list, or every row when nnz == 0).
+// Finishes the rows that cross tiles (their pieces added in tile order) and
+// gives every empty row the value 0.
 template <class Epi, typename AccT>
 __global__ void __launch_bounds__(256)
-    empty_rows_kernel(int count, const int* __restrict__ list, const Epi epi) {
+    spmv_fixup_kernel(const CsrView A, const Epi epi) {
     typename Epi::State est;
     epi.init(est);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
-        epi.apply(est, list ? list[k] : k, AccT(0));
+    const AccT* carry = reinterpret_cast<const AccT*>(A.carry);
+    const int total = A.num_cross + A.num_empty;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        if (k < A.num_cross) {
+            const int4 c = A.cross[k];   // {row, first tile, tiles, 0}
+            AccT sum = carry[2 * c.y + 1];
+            for (int tt = c.y + 1; tt < c.y + c.z; ++tt) sum += carry[2 * tt];
+            epi.apply(est, c.x, sum);
+        } else {
+            epi.apply(est, A.empty_rows[k - A.num_cross], AccT(0));
+        }
+    }
     epi.finish(est);
 }
 
