@@ -124,7 +124,7 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st);
 int device_sm_count(int dev);
 
 constexpr int kSpmvWarps = 8;     // warps per block (each with its own ring)
-constexpr int kSpmvStages = 4;    // ring depth per warp
+constexpr int kSpmvStages = 2;    // ring depth per warp
 
 template <class Epi, typename AccT, typename XT, bool kLo>
 struct SpmvLauncher {

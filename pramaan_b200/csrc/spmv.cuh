@@ -25,13 +25,16 @@
 //   shared-memory ring that its lane 0 fills with 1-D TMA bulk copies
 //   (cp.async.bulk ... mbarrier::complete_tx, L2 evict_first), so warps never
 //   wait on each other: there is no block barrier in the main loop.  Each
-//   lane owns IPT consecutive entries: row ids come from popcounts of the
-//   bitmap (shuffles), the epilogue's vectors for the rows the lane will
-//   finish are prefetched into L2 together with the x gathers, and a
-//   segmented warp scan carries open-row partial sums across lanes.  Rows
-//   that end inside the tile get their epilogue on the spot.  A row that
-//   crosses tiles leaves one partial per tile in carry[] (head piece: the
-//   tile holds its end or a middle part; tail piece: it begins in the tile).
+//   lane owns IPT consecutive entries: it issues its IPT x gathers first,
+//   row ids come from popcounts of the bitmap (shuffles), the epilogue's
+//   vectors for the tile's finished rows are prefetched into L2, products
+//   are accumulated with FMAs, and a segmented warp scan carries open-row
+//   partial sums across lanes.  The rows finished in the tile are
+//   consecutive, so their sums are staged in a per-warp shared buffer and the
+//   epilogue then runs converged, one row per lane, with coalesced loads and
+//   stores.  A row that crosses tiles leaves one partial per tile in carry[]
+//   (head piece: the tile holds its end or a middle part; tail piece: it
+//   begins in the tile).
 //
 // Completion (spmv_fixup_kernel, launched right after on the same stream)
 //   For every crossing row the fixup adds its pieces in tile order and runs
@@ -77,7 +80,8 @@ struct SpmvSmemLayout {
     static constexpr size_t off_flags = slab * kArrays;
     static constexpr size_t off_meta = off_flags + size_t(FW) * 4;
     static constexpr size_t stage_bytes = off_meta + 16;
-    static constexpr size_t warp_bytes = size_t(STAGES) * stage_bytes;
+    static constexpr size_t off_fin = size_t(STAGES) * stage_bytes;        // finished-row values
+    static constexpr size_t warp_bytes = (off_fin + size_t(TW) * sizeof(AccT) + 15) / 16 * 16;
     static constexpr size_t off_bar = size_t(WARPS) * warp_bytes;
     static constexpr size_t bytes = ((off_bar + size_t(WARPS) * STAGES * 8) + 127) / 128 * 128;
     static constexpr unsigned tx_bytes = unsigned(stage_bytes);
@@ -99,7 +103,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 }
 
 template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES>
-__global__ void __launch_bounds__(WARPS * 32)
+__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4))
     spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
                      int* __restrict__ dev_status) {
     using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT>;
@@ -112,10 +116,10 @@ __global__ void __launch_bounds__(WARPS * 32)
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     unsigned char* ring = smem + size_t(warp) * L::warp_bytes;
+    AccT* fin = reinterpret_cast<AccT*>(ring + L::off_fin);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::off_bar) + warp * STAGES;
 
     const int rows_c = A.rows_c;
-    const unsigned last_col = static_cast<unsigned>(A.cols - 1);
 
     typename Epi::State est;
     epi.init(est);
@@ -172,65 +176,55 @@ __global__ void __launch_bounds__(WARPS * 32)
         const int4 meta = *reinterpret_cast<const int4*>(st + L::off_meta);
         const int q0 = lane * IPT;   // tile-local index of my first entry
 
+        // ---- gather x for my entries first: IPT independent loads in flight ----
+        XT xv[IPT];
+        float vv[IPT];
+        float ll[IPT];
+#pragma unroll
+        for (int j = 0; j < IPT; j += 4) {
+            const int4 c4 = *reinterpret_cast<const int4*>(scol + q0 + j);
+            const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
+            xv[j] = __ldg(x + c4.x); xv[j + 1] = __ldg(x + c4.y);
+            xv[j + 2] = __ldg(x + c4.z); xv[j + 3] = __ldg(x + c4.w);
+            vv[j] = v4.x; vv[j + 1] = v4.y; vv[j + 2] = v4.z; vv[j + 3] = v4.w;
+            if constexpr (kLo) {
+                const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
+                ll[j] = l4.x; ll[j + 1] = l4.y; ll[j + 2] = l4.z; ll[j + 3] = l4.w;
+            }
+        }
+
         // ---- row-start bits of my entries and of the entry after them ----
         const uint32_t my = (fl[q0 >> 5] >> (q0 & 31)) & kMask;
         uint32_t next_start;
         if (lane == 31) next_start = meta.y ? 0u : 1u;
         else next_start = (fl[(q0 + IPT) >> 5] >> ((q0 + IPT) & 31)) & 1u;
         const uint32_t ends = (my >> 1) | (next_start << (IPT - 1));   // bit j: entry j ends a row
-        const uint32_t s0 = fl[0] & 1u;                                 // tile's first entry starts a row
+        const int s0 = int(fl[0] & 1u);                                 // tile's first entry starts a row
 
-        // ---- row id of my first entry: first_row + #starts in (0, q0] ----
+        // ---- row ids: first_row + #starts in (0, q] ----
         int incl = __popc(my);
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, incl, d);
             if (lane >= d) incl += v;
         }
-        const int row0 = meta.x + (incl - __popc(my)) + int(my & 1u) - int(s0);
+        const int starts_total = __shfl_sync(0xffffffffu, incl, 31);
+        const int row0 = meta.x + (incl - __popc(my)) + int(my & 1u) - s0;
         const bool head_before = (my & 1u) == 0;   // my first row began before my first entry
 
-        // ---- prefetch the epilogue rows I will finish, then gather x ----
-        const int nends = __popc(ends);
+        // Rows finished in this tile are meta.x .. meta.x + ends_total - 1.  When
+        // the tile's first row began in an earlier tile, its finish here is a
+        // carry piece, so the staged list starts one row later.
+        const int ends_total = starts_total - s0 + (meta.y ? 0 : 1);
+        const int skip = (s0 == 0 && ends_total > 0) ? 1 : 0;
+        const int base = meta.x + skip;
+        int n_fin = ends_total - skip;
+        if (n_fin > rows_c - base) n_fin = rows_c - base;   // virtual padding row
         if constexpr (!kRowMap) {
-            if (nends > 0) {
-                const int r_last = row0 + nends - 1;
-                if (row0 < rows_c) epi.prefetch(row0);
-                if (r_last != row0 && r_last < rows_c) epi.prefetch(r_last);
-            }
-        }
-        AccT p[IPT];
-#pragma unroll
-        for (int j = 0; j < IPT; j += 4) {
-            const int4 c4 = *reinterpret_cast<const int4*>(scol + q0 + j);
-            const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
-            const int cc[4] = {c4.x, c4.y, c4.z, c4.w};
-            const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
-            float ll[4] = {0.f, 0.f, 0.f, 0.f};
-            if constexpr (kLo) {
-                const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
-                ll[0] = l4.x; ll[1] = l4.y; ll[2] = l4.z; ll[3] = l4.w;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                unsigned ci = static_cast<unsigned>(cc[q]);
-                ci = ci < last_col ? ci : last_col;   // never gather out of bounds
-                const XT xv = __ldg(x + ci);
-                if constexpr (kLo) {
-                    p[j + q] = (static_cast<AccT>(vv[q]) + static_cast<AccT>(ll[q])) * static_cast<AccT>(xv);
-                } else {
-                    p[j + q] = static_cast<AccT>(vv[q]) * static_cast<AccT>(xv);
-                }
-            }
+            for (int k = lane * 8; k < n_fin; k += 256) epi.prefetch(base + k);
         }
 
-        auto emit = [&](int row_c, AccT v) {
-            if (row_c >= rows_c) return;   // virtual padding row
-            const int r = kRowMap ? A.row_map[row_c] : row_c;
-            epi.apply(est, r, v);
-        };
-
-        // ---- walk my entries; finish the rows that end here ----
+        // ---- walk my entries; stage the rows that end here ----
         AccT acc = AccT(0);
         int cur = row0;
         int nemit = 0;
@@ -238,10 +232,14 @@ __global__ void __launch_bounds__(WARPS * 32)
         bool head_pending = false;
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
-            acc += p[j];
+            if constexpr (kLo) {
+                acc = fma(static_cast<AccT>(vv[j]) + static_cast<AccT>(ll[j]), static_cast<AccT>(xv[j]), acc);
+            } else {
+                acc = fma(static_cast<AccT>(vv[j]), static_cast<AccT>(xv[j]), acc);
+            }
             if ((ends >> j) & 1u) {
                 if (nemit == 0 && head_before) { head_acc = acc; head_pending = true; }
-                else emit(cur, acc);
+                else fin[cur - base] = acc;
                 ++nemit;
                 ++cur;
                 acc = AccT(0);
@@ -260,19 +258,24 @@ __global__ void __launch_bounds__(WARPS * 32)
         AccT carry_in = __shfl_up_sync(0xffffffffu, v, 1);   // partial of the row open at q0
         if (lane == 0) carry_in = AccT(0);
 
-        const bool first_began_before = s0 == 0;   // tile's first row began in an earlier tile
         if (head_pending) {
             const AccT tot = head_acc + carry_in;
-            if (row0 == meta.x && first_began_before) carry[2 * t] = tot;   // last piece of a crossing row
-            else emit(row0, tot);
+            if (row0 == meta.x && s0 == 0) carry[2 * t] = tot;   // last piece of a crossing row
+            else fin[row0 - base] = tot;
         }
         if (lane == 31 && meta.y) {   // the tile's last row continues into the next tile
             const AccT tot = nemit > 0 ? acc : carry_in + acc;
-            if (cur == meta.x && first_began_before) carry[2 * t] = tot;    // middle piece
-            else carry[2 * t + 1] = tot;                                    // first piece
+            if (cur == meta.x && s0 == 0) carry[2 * t] = tot;    // middle piece
+            else carry[2 * t + 1] = tot;                         // first piece
         }
+        __syncwarp();
 
-        __syncwarp();   // every lane is done with stage s
+        // ---- epilogue over the finished rows, one row per lane (coalesced) ----
+        for (int k = lane; k < n_fin; k += 32) {
+            const int rc = base + k;
+            epi.apply(est, kRowMap ? A.row_map[rc] : rc, fin[k]);
+        }
+        __syncwarp();   // stage s and the staged values are free for reuse
         if (lane == 0 && i + STAGES < mine) {
             fence_proxy_async_smem();
             issue(i + STAGES);

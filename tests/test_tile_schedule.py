@@ -68,6 +68,19 @@ def emulate(rp, prod, T=TILE, IPT=8):
         fl = flags[t * T:(t + 1) * T]
         pr = padded[t * T:(t + 1) * T]
         s0 = int(fl[0])
+        # staged finished rows: meta.x + skip .. , n_fin of them (kernel: base / n_fin)
+        ends_total = int(fl.sum()) - s0 + (0 if cont else 1)
+        skip = 1 if (s0 == 0 and ends_total > 0) else 0
+        base = fr + skip
+        n_fin = min(ends_total - skip, rows_c - base)
+        fin = [None] * T
+
+        def stage(row_c, v):
+            k = row_c - base
+            assert 0 <= k < T, (k, T)
+            assert fin[k] is None, "staged twice"
+            fin[k] = v
+
         st = []
         for lane in range(lanes):
             q0 = lane * IPT
@@ -83,7 +96,7 @@ def emulate(rp, prod, T=TILE, IPT=8):
                     if nemit == 0 and head_before:
                         head_acc, head_pending = acc, True
                     else:
-                        emit(cur, acc)
+                        stage(cur, acc)
                     nemit += 1
                     cur += 1
                     acc = 0
@@ -101,13 +114,20 @@ def emulate(rp, prod, T=TILE, IPT=8):
                 if s["row0"] == fr and s0 == 0:
                     carry[(t, 0)] = tot
                 else:
-                    emit(s["row0"], tot)
+                    stage(s["row0"], tot)
             if lane == lanes - 1 and cont:
                 tot = s["acc"] if s["nemit"] > 0 else carry_in + s["acc"]
                 if s["cur"] == fr and s0 == 0:
                     carry[(t, 0)] = tot
                 else:
                     carry[(t, 1)] = tot
+        # converged epilogue over the staged rows
+        for k in range(max(n_fin, 0)):
+            assert fin[k] is not None, (t, k, n_fin)
+            emit(base + k, fin[k])
+        # only the virtual padding row may be staged beyond n_fin
+        for k in range(max(n_fin, 0), T):
+            assert fin[k] is None or base + k >= rows_c
     # fixup: crossing rows in tile order, then empty rows
     for row, t0, cnt in F["cross"]:
         s = carry[(t0, 1)]
