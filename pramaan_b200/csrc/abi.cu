@@ -100,12 +100,15 @@ void spmv_harness(const int32_t* row_ptr, const int32_t* col_idx, const float* v
     else
         PB_CUDA_CHECK(cudaMemsetAsync(dx.get(), 0, dx.bytes(), st));
     EpiStore<float, float> epi{dy.get()};
+    SpmvLauncher<EpiStore<float, float>, float, float, false>::blocks_per_sm(dev);
     if (!transpose) {
+        A.pack(st);
         SpmvLauncher<EpiStore<float, float>, float, float, false>::launch(A.view(false), dx.get(), epi,
                                                                          flag.get(), st, dev);
     } else {
         CsrDevice AT;
         csr_transpose(A, AT, st);
+        AT.pack(st);
         SpmvLauncher<EpiStore<float, float>, float, float, false>::launch(AT.view(false), dx.get(),
                                                                          epi, flag.get(), st, dev);
         PB_CUDA_CHECK(cudaStreamSynchronize(st));

@@ -174,6 +174,26 @@ __global__ void keys_to_rowptr_kernel(const int* __restrict__ keys, int nnz, int
     }
 }
 
+// One block per tile: interleave the flat arrays into the tile record.
+__global__ void pack_kernel(const int* __restrict__ col, const float* __restrict__ val,
+                            const uint32_t* __restrict__ flags, const int4* __restrict__ meta,
+                            int tiles, unsigned char* __restrict__ rec) {
+    constexpr int TW = TileRec::TW, FW = TileRec::FW;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        unsigned char* r = rec + size_t(t) * TileRec::bytes;
+        int* rc = reinterpret_cast<int*>(r + TileRec::off_col);
+        float* rv = reinterpret_cast<float*>(r + TileRec::off_val);
+        uint32_t* rf = reinterpret_cast<uint32_t*>(r + TileRec::off_flags);
+        const size_t base = size_t(t) * TW;
+        for (int k = threadIdx.x; k < TW; k += blockDim.x) {
+            rc[k] = col[base + k];
+            rv[k] = val[base + k];
+        }
+        for (int k = threadIdx.x; k < FW; k += blockDim.x) rf[k] = flags[size_t(t) * FW + k];
+        if (threadIdx.x == 0) *reinterpret_cast<int4*>(r + TileRec::off_meta) = meta[t];
+    }
+}
+
 __global__ void permute_kernel(const int* __restrict__ perm, const int* __restrict__ row_of,
                                const float* __restrict__ val, const float* __restrict__ lo,
                                int nnz, int* __restrict__ t_col, float* __restrict__ t_val,
@@ -188,12 +208,31 @@ __global__ void permute_kernel(const int* __restrict__ perm, const int* __restri
 
 }  // namespace
 
+void CsrDevice::pack(cudaStream_t st) {
+    if (packed) return;
+    if (num_tiles > 0) {
+        rec.alloc(size_t(num_tiles) * TileRec::bytes);
+        const int grid = num_tiles < 65535 * 4 ? num_tiles : 65535 * 4;
+        pack_kernel<<<grid, 256, 0, st>>>(col.get(), val.get(), flags.get(), meta.get(), num_tiles,
+                                          rec.get());
+        PB_CUDA_CHECK(cudaGetLastError());
+        PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    col.reset();
+    val.reset();
+    flags.reset();
+    meta.reset();
+    packed = true;
+}
+
 void CsrDevice::allocate(int rows_, int cols_, int nnz_, bool lo) {
     if (rows_ < 0 || cols_ < 0 || nnz_ < 0) throw InvalidArgument("negative CSR dimension");
     rows = rows_; cols = cols_; nnz = nnz_;
     num_tiles = nnz > 0 ? ceil_div(nnz, kSpmvTile) : 0;
     nnz_pad = num_tiles * kSpmvTile;
     has_lo = lo;
+    packed = false;
+    rec.reset();
     row_ptr.alloc(size_t(rows) + 1);
     col.alloc(size_t(nnz_pad));
     val.alloc(size_t(nnz_pad));

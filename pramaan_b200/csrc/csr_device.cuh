@@ -3,23 +3,28 @@
 //
 // Layout in HBM (one operand; A and its stored transpose each get one):
 //   row_ptr    int32 [rows + 1]        the CSR row pointer as given
-//   col        int32 [nnz_pad]         pad entries: col 0
-//   val        fp32  [nnz_pad]         value rounded to nearest FP32, pad 0
+//   rec        tile records [tiles]    per tile: col int32[512] (pad: 0),
+//                                      val fp32[512] (FP32-rounded, pad: 0),
+//                                      flags u32[16] (bit q: entry q starts a
+//                                      non-empty row), meta int4
+//                                      {first_row, tail_continues, 0, 0}
 //   val_lo     fp32  [nnz_pad]         FP32(value - val), kept only when some
 //                                      value is not exactly representable
-//   flags      u32   [nnz_pad / 32]    bit q: entry q starts a non-empty row
-//   meta       int4  [tiles]           {first_row, tail_continues, 0, 0}
 //   row_map    int32 [rows_c]          original row of each non-empty row (only
 //                                      when empty rows exist)
 //   empty_rows int32 [rows - rows_c]   rows without entries
 //   cross      int4  [crossing rows]   {row, first tile, tiles, 0} per row spanning tiles
 //   carry      f64   [2 * tiles]       per-tile partials of crossing rows (scratch)
-// nnz_pad is a multiple of the tile (256 entries), and every array starts on
-// a 256-byte boundary (cudaMalloc), so each tile's slabs are 16-byte aligned
-// for the bulk copies.
+// nnz_pad is a multiple of the tile (512 entries); records are 4176 bytes and
+// every array starts on a 256-byte boundary (cudaMalloc), so each record and
+// each tile's val_lo slab is 16-byte aligned for the bulk copies.  While an
+// operand is being built it is held as flat col / val / flags / meta arrays
+// (what the transpose and the step-size pass read); pack() then interleaves
+// them into the records and frees the flat copies.
 #pragma once
 
 #include <atomic>
+#include <stdexcept>
 #include <cstddef>
 #include <vector>
 
@@ -69,19 +74,21 @@ public:
     int rows = 0, cols = 0, nnz = 0, nnz_pad = 0, num_tiles = 0;
     int rows_c = 0, num_empty = 0, num_cross = 0;
     bool has_lo = false;
+    bool packed = false;
     DevBuf<int> row_ptr, col, row_map, empty_rows;
     DevBuf<float> val, val_lo;
     DevBuf<uint32_t> flags;
     DevBuf<int4> meta, cross;
+    DevBuf<unsigned char> rec;
     DevBuf<double> carry;
 
     CsrView view(bool with_lo) const {
         CsrView v;
         v.rows = rows; v.cols = cols; v.nnz = nnz; v.nnz_pad = nnz_pad; v.num_tiles = num_tiles;
         v.rows_c = rows_c; v.num_empty = num_empty; v.num_cross = num_cross;
-        v.col = col.get(); v.val = val.get();
+        if (!packed && num_tiles > 0) throw std::logic_error("CsrDevice::view before pack()");
+        v.rec = rec.get();
         v.val_lo = (with_lo && has_lo) ? val_lo.get() : nullptr;
-        v.flags = flags.get(); v.meta = meta.get();
         v.row_map = row_map.get(); v.empty_rows = empty_rows.get();
         v.cross = cross.get(); v.carry = carry.get();
         return v;
@@ -98,10 +105,12 @@ public:
     void allocate(int rows_, int cols_, int nnz_, bool lo);
     // Builds flags / meta / row compaction / crossing rows from row_ptr.
     void finalize(cudaStream_t st);
+    // Interleaves col / val / flags / meta into tile records and frees them.
+    void pack(cudaStream_t st);
     size_t device_bytes() const {
         return row_ptr.bytes() + col.bytes() + row_map.bytes() + empty_rows.bytes() +
                val.bytes() + val_lo.bytes() + flags.bytes() + meta.bytes() + cross.bytes() +
-               carry.bytes();
+               rec.bytes() + carry.bytes();
     }
 };
 
@@ -123,7 +132,7 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st);
 // ---------------------------------------------------------------------------
 int device_sm_count(int dev);
 
-constexpr int kSpmvWarps = 8;     // warps per block (each with its own ring)
+constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
 
 template <class Epi, typename AccT, typename XT, bool kLo>

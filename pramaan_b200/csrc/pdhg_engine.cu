@@ -177,6 +177,9 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
         PB_CUDA_CHECK(cudaGetLastError());
         PB_CUDA_CHECK(cudaMemsetAsync(y_.get(), 0, size_t(m_) * 4, st_));
     }
+    // The step sizes above read the flat operands; interleave them into tile records now.
+    A_.pack(st_);
+    AT_.pack(st_);
     // Occupancy queries / smem attributes before any graph capture.
     SpmvLauncher<EpiDualRef, float, float, false>::blocks_per_sm(dev_);
     SpmvLauncher<EpiPrimalRef, float, float, false>::blocks_per_sm(dev_);

@@ -8,12 +8,15 @@
 //
 // Tiled operand format (built once per matrix, see csr_device.cu)
 //   The non-zeros are cut into tiles of TW = 32*IPT consecutive entries, one
-//   tile per warp at a time.  Per tile, four slabs sit at 16-byte aligned
-//   offsets:
+//   tile per warp at a time.  Each tile is ONE contiguous record, so a single
+//   ~4 KB bulk copy moves it (copies of 2 KB or less stream at well under
+//   half of HBM bandwidth on B200; 4 KB and up reach it):
 //     col   int32[TW]     column indices
-//     val   fp32 [TW]     values (FP32-rounded)      [+ val_lo fp32[TW]]
+//     val   fp32 [TW]     values (FP32-rounded)
 //     flags u32 [TW/32]   bit q set <=> entry q starts a row
 //     meta  int4          {first_row, tail_continues, 0, 0}
+//   The FP32 remainders val_lo (value - val), when present, stay in a flat
+//   array and travel in a second copy, only for the FP64 products.
 //   Empty rows are compacted out (an optional row_map gives the original row
 //   of every compacted row) and the padding after the last entry forms a
 //   virtual row that is never emitted, so row ids follow from the bitmap
@@ -47,8 +50,20 @@
 
 namespace pb {
 
-constexpr int kSpmvIpt = 8;                  // entries per lane
+constexpr int kSpmvIpt = 16;                 // entries per lane
 constexpr int kSpmvTile = 32 * kSpmvIpt;     // entries per warp-tile (format unit)
+
+// Byte layout of one tile record.
+struct TileRec {
+    static constexpr int TW = kSpmvTile;
+    static constexpr int FW = TW / 32;
+    static constexpr size_t off_col = 0;
+    static constexpr size_t off_val = size_t(TW) * 4;
+    static constexpr size_t off_flags = size_t(TW) * 8;
+    static constexpr size_t off_meta = off_flags + size_t(FW) * 4;
+    static constexpr size_t bytes = off_meta + 16;
+    static_assert(bytes % 16 == 0, "tile records must be 16-byte multiples");
+};
 
 // Device view of one CSR operand in the tiled format.
 struct CsrView {
@@ -58,11 +73,8 @@ struct CsrView {
     int rows_c = 0;        // non-empty (compacted) rows
     int num_empty = 0;     // rows without entries
     int num_cross = 0;     // rows spanning more than one tile
-    const int* col = nullptr;         // nnz_pad
-    const float* val = nullptr;       // nnz_pad
-    const float* val_lo = nullptr;    // nnz_pad or null
-    const uint32_t* flags = nullptr;  // nnz_pad / 32
-    const int4* meta = nullptr;       // num_tiles: {first_row, tail_continues, 0, 0}
+    const unsigned char* rec = nullptr;   // num_tiles tile records (TileRec)
+    const float* val_lo = nullptr;        // nnz_pad or null
     const int* row_map = nullptr;     // rows_c (null: identity)
     const int* empty_rows = nullptr;  // num_empty
     const int4* cross = nullptr;      // num_cross: {original row, first tile, tiles, 0}
@@ -72,21 +84,18 @@ struct CsrView {
 template <int WARPS, int STAGES, bool kLo, typename AccT>
 struct SpmvSmemLayout {
     static constexpr int TW = kSpmvTile;
-    static constexpr int FW = TW / 32;
-    static constexpr int kArrays = kLo ? 3 : 2;
-    static constexpr size_t slab = size_t(TW) * 4;
-    static constexpr size_t off_val = slab;
-    static constexpr size_t off_lo = 2 * slab;
-    static constexpr size_t off_flags = slab * kArrays;
-    static constexpr size_t off_meta = off_flags + size_t(FW) * 4;
-    static constexpr size_t stage_bytes = off_meta + 16;
+    static constexpr int FW = TileRec::FW;
+    static constexpr size_t off_val = TileRec::off_val;
+    static constexpr size_t off_flags = TileRec::off_flags;
+    static constexpr size_t off_meta = TileRec::off_meta;
+    static constexpr size_t off_lo = TileRec::bytes;                         // kLo only
+    static constexpr size_t stage_bytes = TileRec::bytes + (kLo ? size_t(TW) * 4 : 0);
     static constexpr size_t off_fin = size_t(STAGES) * stage_bytes;        // finished-row values
     static constexpr size_t warp_bytes = (off_fin + size_t(TW) * sizeof(AccT) + 15) / 16 * 16;
     static constexpr size_t off_bar = size_t(WARPS) * warp_bytes;
     static constexpr size_t bytes = ((off_bar + size_t(WARPS) * STAGES * 8) + 127) / 128 * 128;
     static constexpr unsigned tx_bytes = unsigned(stage_bytes);
-    static_assert(stage_bytes % 16 == 0 && (size_t(FW) * 4) % 16 == 0,
-                  "TMA slabs must be 16-byte multiples");
+    static_assert(stage_bytes % 16 == 0, "TMA copies must be 16-byte multiples");
 };
 
 // Epilogue concept:
@@ -103,7 +112,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 }
 
 template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES>
-__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4))
+__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS)
     spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
                      int* __restrict__ dev_status) {
     using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT>;
@@ -143,11 +152,8 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4))
         unsigned char* st = ring + size_t(s) * L::stage_bytes;
         const size_t off = size_t(t) * TW;
         mbar_arrive_expect_tx(&bar[s], L::tx_bytes);
-        tma_bulk_g2s(st, A.col + off, TW * 4, &bar[s], policy);
-        tma_bulk_g2s(st + L::off_val, A.val + off, TW * 4, &bar[s], policy);
+        tma_bulk_g2s(st, A.rec + size_t(t) * TileRec::bytes, unsigned(TileRec::bytes), &bar[s], policy);
         if constexpr (kLo) tma_bulk_g2s(st + L::off_lo, A.val_lo + off, TW * 4, &bar[s], policy);
-        tma_bulk_g2s(st + L::off_flags, A.flags + size_t(t) * FW, FW * 4, &bar[s], policy);
-        tma_bulk_g2s(st + L::off_meta, A.meta + t, 16, &bar[s], policy);
     };
 
     if (lane == 0) {

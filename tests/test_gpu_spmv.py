@@ -15,7 +15,7 @@ from lp_cases import random_csr
 from pramaan_b200 import launch_spmv, launch_spmv_t
 
 pytestmark = pytest.mark.gpu
-TILE = 256
+TILE = 512
 
 
 def close(gpu, ref):

@@ -13,7 +13,7 @@ sums are exact.
 import numpy as np
 import pytest
 
-TILE = 256   # 32 lanes x 8 entries, the format unit of the library
+TILE = 512   # 32 lanes x 16 entries, the format unit of the library
 
 
 def build_format(rp, T):
@@ -142,10 +142,10 @@ def emulate(rp, prod, T=TILE, IPT=8):
     return out
 
 
-def check(rp, rng, T=TILE):
+def check(rp, rng, T=TILE, IPT=8):
     nnz = int(rp[-1])
     prod = rng.integers(-3, 4, size=nnz)
-    out = emulate(np.asarray(rp, np.int64), prod, T=T)
+    out = emulate(np.asarray(rp, np.int64), prod, T=T, IPT=IPT)
     m = len(rp) - 1
     assert sorted(out) == list(range(m))
     for r in range(m):
@@ -183,4 +183,4 @@ def test_schedule_library_tile_size():
                         rng.integers(0, 9, 200)])
     rp = np.zeros(len(L) + 1, np.int64)
     rp[1:] = np.cumsum(L)
-    check(rp, rng, T=TILE)
+    check(rp, rng, T=TILE, IPT=16)
