@@ -73,6 +73,7 @@ class CsrDevice {
 public:
     int rows = 0, cols = 0, nnz = 0, nnz_pad = 0, num_tiles = 0;
     int rows_c = 0, num_empty = 0, num_cross = 0;
+    int tuned_blocks_per_sm = 0;   // set by the launch autotuner (0: default)
     bool has_lo = false;
     bool packed = false;
     DevBuf<int> row_ptr, col, row_map, empty_rows;
@@ -86,6 +87,7 @@ public:
         CsrView v;
         v.rows = rows; v.cols = cols; v.nnz = nnz; v.nnz_pad = nnz_pad; v.num_tiles = num_tiles;
         v.rows_c = rows_c; v.num_empty = num_empty; v.num_cross = num_cross;
+        v.blocks_per_sm = tuned_blocks_per_sm;
         if (!packed && num_tiles > 0) throw std::logic_error("CsrDevice::view before pack()");
         v.rec = rec.get();
         v.val_lo = (with_lo && has_lo) ? val_lo.get() : nullptr;
@@ -142,6 +144,11 @@ struct SpmvLauncher {
     static constexpr auto kernel() {
         return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvWarps, kSpmvStages>;
     }
+    // Default resident blocks per SM: as many as fit in ~132 KB of shared
+    // memory, which leaves ~100 KB of L1 for outstanding gather misses.
+    static constexpr int kTargetBlocks =
+        int((132 * 1024) / (L::bytes + 1024)) > 0 ? int((132 * 1024) / (L::bytes + 1024)) : 1;
+
     template <bool kRowMap>
     static int blocks_per_sm_impl(int dev) {
         static std::atomic<int> cache[64];
@@ -150,6 +157,12 @@ struct SpmvLauncher {
         if (v > 0) return v;
         PB_CUDA_CHECK(cudaFuncSetAttribute(kernel<kRowMap>(),
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes)));
+        // Carve-out for kTargetBlocks blocks (percent of the 228 KB maximum).
+        const long long need = (long long)kTargetBlocks * (L::bytes + 1024);
+        int pct = int((need * 100 + 228 * 1024 - 1) / (228 * 1024));
+        pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+        PB_CUDA_CHECK(cudaFuncSetAttribute(kernel<kRowMap>(),
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         int nb = 0;
         PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel<kRowMap>(),
                                                                     kSpmvWarps * 32, L::bytes));
@@ -157,22 +170,29 @@ struct SpmvLauncher {
         cache[dev].store(nb, std::memory_order_relaxed);
         return nb;
     }
-    // Queries occupancy (and sets the shared-memory attribute) for both
+    // Queries occupancy (and sets the shared-memory attributes) for both
     // variants; call before any stream capture.
     static int blocks_per_sm(int dev) {
         blocks_per_sm_impl<true>(dev);
         return blocks_per_sm_impl<false>(dev);
+    }
+    // Grid for one launch: A.blocks_per_sm (autotuned) or the default target,
+    // never more than fit, never more blocks than tile groups.
+    static int grid_for(const CsrView& A, int dev) {
+        const bool mapped = A.row_map != nullptr;
+        const int occ = mapped ? blocks_per_sm_impl<true>(dev) : blocks_per_sm_impl<false>(dev);
+        int bps = A.blocks_per_sm > 0 ? A.blocks_per_sm : kTargetBlocks;
+        bps = bps < occ ? bps : occ;
+        const long long cap = (long long)bps * device_sm_count(dev);
+        const long long need = (A.num_tiles + kSpmvWarps - 1) / kSpmvWarps;
+        return int(need < cap ? need : cap);
     }
     static void launch(const CsrView& A, const XT* x, const Epi& epi, int* dev_status,
                        cudaStream_t st, int dev) {
         if (A.rows <= 0) return;
         if (A.num_tiles > 0) {
             const bool mapped = A.row_map != nullptr;
-            const long long cap = (long long)(mapped ? blocks_per_sm_impl<true>(dev)
-                                                     : blocks_per_sm_impl<false>(dev)) *
-                                  device_sm_count(dev);
-            const long long need = (A.num_tiles + kSpmvWarps - 1) / kSpmvWarps;
-            const int grid = int(need < cap ? need : cap);
+            const int grid = grid_for(A, dev);
             if (mapped) {
                 auto k = kernel<true>();
                 k<<<grid, kSpmvWarps * 32, L::bytes, st>>>(A, x, epi, dev_status);

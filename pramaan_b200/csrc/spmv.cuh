@@ -23,6 +23,16 @@
 //   alone: row(q) = first_row + #starts in (0, q].  The kernel never reads
 //   row_ptr.
 //
+// What bounds it
+//   On a random sparsity pattern every entry costs one 4-byte gather of x
+//   from L2, and B200 serves random gathers at about one L1 request per clock
+//   per SM (~288 G/s per GPU measured) whatever the cache operator, while
+//   the matrix stream itself needs well under half of HBM bandwidth at that
+//   rate.  Outstanding gather misses occupy L1 lines, so the kernel runs with
+//   a shared-memory carve-out sized for 3-4 blocks per SM (leaving ~100 KB of
+//   L1) rather than the largest carve-out: with the L1 squeezed to ~40 KB
+//   the same kernel runs at half the gather rate.
+//
 // Schedule (spmv_warp_kernel)
 //   A persistent grid walks the tiles; every warp owns a private STAGES-deep
 //   shared-memory ring that its lane 0 fills with 1-D TMA bulk copies
@@ -73,6 +83,7 @@ struct CsrView {
     int rows_c = 0;        // non-empty (compacted) rows
     int num_empty = 0;     // rows without entries
     int num_cross = 0;     // rows spanning more than one tile
+    int blocks_per_sm = 0; // grid = blocks_per_sm x SMs (0: library default)
     const unsigned char* rec = nullptr;   // num_tiles tile records (TileRec)
     const float* val_lo = nullptr;        // nnz_pad or null
     const int* row_map = nullptr;     // rows_c (null: identity)
@@ -190,8 +201,10 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
         for (int j = 0; j < IPT; j += 4) {
             const int4 c4 = *reinterpret_cast<const int4*>(scol + q0 + j);
             const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
-            xv[j] = __ldg(x + c4.x); xv[j + 1] = __ldg(x + c4.y);
-            xv[j + 2] = __ldg(x + c4.z); xv[j + 3] = __ldg(x + c4.w);
+            // ld.global.cg: the gathers are served by L2; caching them in L1
+            // only evicts lines other warps are waiting on.
+            xv[j] = __ldcg(x + c4.x); xv[j + 1] = __ldcg(x + c4.y);
+            xv[j + 2] = __ldcg(x + c4.z); xv[j + 3] = __ldcg(x + c4.w);
             vv[j] = v4.x; vv[j + 1] = v4.y; vv[j + 2] = v4.z; vv[j + 3] = v4.w;
             if constexpr (kLo) {
                 const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
