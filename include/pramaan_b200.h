@@ -140,6 +140,27 @@ PRAMAAN_API int pramaan_launch_pdhg_iteration(float* h_x, float* h_y, const floa
                                   const float* h_Ax_bar, const float* h_b, int32_t n, int32_t m,
                                   float tau, float sigma);
 
+/* y[m] = A x for a CSR that already lives in device memory, allocating
+ * nothing.  This entry point has no counterpart in the reference.  It exists
+ * for callers that cannot call cudaMalloc where they need the product: drivers
+ * that size all device memory up front under a fixed budget (branch-and-bound,
+ * rolling-horizon loops), code running while a stream is captured into a CUDA
+ * graph, and hosts that own the device memory pool.  All pointers are device
+ * pointers owned by the caller (row_ptr[m+1], col_idx[nnz], values[nnz], x[n],
+ * y[m]); the work is queued on `stream` (a cudaStream_t, NULL for the legacy
+ * default stream) and the call returns without waiting.  Partial sums of rows
+ * that cross 2048-entry tiles go to a 512 KiB scratch array compiled into the
+ * library (a file-scope __device__ array, held by every GPU that loads the
+ * library until exit), which limits nnz to 134,217,728; larger inputs are
+ * rejected with PRAMAAN_ERR_INVALID_ARGUMENT.  Every call shares that array:
+ * calls on one stream are ordered, calls that overlap on the GPU race.  The
+ * first call on a device looks up the array's device address (no allocation).
+ * The CSR is not validated; out-of-range column indices are clamped so they
+ * never read outside x. */
+PRAMAAN_API int pramaan_spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_idx,
+                                     const float* d_values, int32_t m, int32_t n, int32_t nnz,
+                                     const float* d_x, float* d_y, void* stream);
+
 /* ---- device-resident session (benchmarks and advanced callers) ----------- */
 
 typedef struct pramaan_pdhg_session pramaan_pdhg_session;

@@ -57,6 +57,7 @@ SIGNATURES = [
     ("pramaan_launch_spmv", C.c_int, [P, P, P, i32, P, P, i32, i32]),
     ("pramaan_launch_spmv_t", C.c_int, [P, P, P, i32, P, P, i32, i32]),
     ("pramaan_launch_pdhg_iteration", C.c_int, [P, P, P, P, P, i32, i32, f32, f32]),
+    ("pramaan_spmv_noalloc", C.c_int, [P, P, P, i32, i32, i32, P, P, P]),
     ("pramaan_session_create", C.c_int, [C.POINTER(CLp), C.POINTER(COptions), C.POINTER(P)]),
     ("pramaan_session_destroy", C.c_int, [P]),
     ("pramaan_session_iterate", C.c_int, [P, i32]),

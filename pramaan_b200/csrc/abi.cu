@@ -18,6 +18,13 @@ struct pramaan_pdhg_session {
 };
 
 namespace pb {
+// noalloc.cu
+void spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_idx, const float* d_values,
+                  int32_t m, int32_t n, int32_t nnz, const float* d_x, float* d_y,
+                  cudaStream_t stream);
+}  // namespace pb
+
+namespace pb {
 namespace {
 
 thread_local std::string g_last_error;
@@ -234,6 +241,15 @@ int pramaan_launch_pdhg_iteration(float* h_x, float* h_y, const float* h_gradien
         if (n > 0) PB_CUDA_CHECK(cudaMemcpyAsync(h_x, dx.get(), size_t(n) * 4, cudaMemcpyDeviceToHost, st));
         if (m > 0) PB_CUDA_CHECK(cudaMemcpyAsync(h_y, dy.get(), size_t(m) * 4, cudaMemcpyDeviceToHost, st));
         PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    });
+}
+
+int pramaan_spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_idx, const float* d_values,
+                         int32_t m, int32_t n, int32_t nnz, const float* d_x, float* d_y,
+                         void* stream) {
+    return guarded([&] {
+        spmv_noalloc(d_row_ptr, d_col_idx, d_values, m, n, nnz, d_x, d_y,
+                     static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -184,3 +184,126 @@ def test_schedule_library_tile_size():
     rp = np.zeros(len(L) + 1, np.int64)
     rp[1:] = np.cumsum(L)
     check(rp, rng, T=TILE, IPT=16)
+
+
+# ---------------------------------------------------------------------------
+# The allocation-free product (noalloc.cu): block merge-path over a plain CSR,
+# rows found by binary search, crossing rows finished by a fixup pass.
+# ---------------------------------------------------------------------------
+def emulate_noalloc(rp, prod, T=64, IPT=8):
+    m = len(rp) - 1
+    nnz = int(rp[-1])
+    nt = (nnz + T - 1) // T
+    pad = nt * T
+
+    def rp_at(r):
+        return int(rp[r]) if r <= m else pad
+
+    def row_holding(q):
+        lo, hi = 0, m
+        while lo < hi:
+            mid = (lo + hi + 1) >> 1
+            if rp[mid] <= q:
+                lo = mid
+            else:
+                hi = mid - 1
+        return lo
+
+    y = {}
+    carry = {}
+    B = T // IPT
+    padded = np.zeros(pad, np.int64)
+    padded[:nnz] = prod
+
+    def put(r, v):
+        assert 0 <= r < m and r not in y, r
+        y[r] = v
+
+    for t in range(nt):
+        tile_base, tile_end = t * T, t * T + T
+        r_lo = 0 if t == 0 else row_holding(tile_base)
+        r_hi = m if t == nt - 1 else row_holding(tile_end)
+        lanes = []
+        for tid in range(B):
+            k0, k1 = tile_base + tid * IPT, tile_base + tid * IPT + IPT
+            lo, hi = r_lo, r_hi
+            while lo < hi:
+                mid = (lo + hi) >> 1
+                if rp_at(mid + 1) > k0:
+                    hi = mid
+                else:
+                    lo = mid + 1
+            r = 0 if (t == 0 and tid == 0) else lo
+            st = dict(acc=0, nemit=0, head_row=-1, head_acc=0)
+
+            def finish(row):
+                if st["nemit"] == 0 and rp_at(row) < k0:
+                    st["head_row"], st["head_acc"] = row, st["acc"]
+                else:
+                    put(row, st["acc"])
+                st["nemit"] += 1
+                st["acc"] = 0
+
+            for j in range(IPT):
+                while r < m and r <= r_hi and rp_at(r + 1) <= k0 + j:
+                    finish(r)
+                    r += 1
+                st["acc"] += int(padded[k0 + j])
+            while r < m and r <= r_hi and rp_at(r + 1) <= k1:
+                finish(r)
+                r += 1
+            lanes.append((r, st["acc"], st))
+        # segmented scan by tail row; exclusive value per lane
+        incl = []
+        for i, (krow, kval, _) in enumerate(lanes):
+            if i > 0 and incl[-1][0] == krow:
+                incl.append((krow, incl[-1][1] + kval))
+            else:
+                incl.append((krow, kval))
+        for i, (krow, kval, st) in enumerate(lanes):
+            erow, ev = incl[i - 1] if i > 0 else (-1, 0)
+            if st["head_row"] >= 0:
+                tot = st["head_acc"] + (ev if erow == st["head_row"] else 0)
+                if rp_at(st["head_row"]) >= tile_base:
+                    put(st["head_row"], tot)
+                else:
+                    carry[2 * t] = tot
+            if i == B - 1 and krow < m and rp_at(krow) < tile_end and rp_at(krow + 1) > tile_end:
+                carry[2 * t + (1 if rp_at(krow) >= tile_base else 0)] = incl[i][1]
+    for t in range(nt - 1):
+        R = row_holding(t * T + T - 1)
+        if R >= m:
+            continue
+        start, end = rp_at(R), rp_at(R + 1)
+        if start < t * T or end <= t * T + T:
+            continue
+        s = carry[2 * t + 1]
+        for tt in range(t + 1, (end - 1) // T + 1):
+            s += carry[2 * tt]
+        put(R, s)
+    return y
+
+
+@pytest.mark.parametrize("mode", range(4))
+def test_noalloc_schedule_random_structures(mode):
+    rng = np.random.default_rng(500 + mode)
+    for trial in range(200):
+        m = int(rng.integers(1, 50))
+        if mode == 0:
+            L = rng.integers(0, 5, m)
+        elif mode == 1:
+            L = rng.integers(0, 200, m)
+        elif mode == 2:
+            L = rng.choice([0, 1, 63, 64, 65, 128, 8, 7], m)
+        else:
+            L = np.where(rng.random(m) < 0.1, rng.integers(300, 700, m), rng.integers(0, 3, m))
+        rp = np.zeros(m + 1, np.int64)
+        rp[1:] = np.cumsum(L)
+        if rp[-1] == 0:
+            continue
+        prod = rng.integers(-3, 4, size=int(rp[-1]))
+        y = emulate_noalloc(rp, prod)
+        for r in range(m):
+            expect = int(prod[rp[r]:rp[r + 1]].sum())
+            assert r in y, (trial, r)          # every row is written, empty rows with 0
+            assert y[r] == expect, (trial, r)
