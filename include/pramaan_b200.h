@@ -53,7 +53,10 @@ extern "C" {
 
 /* ---- algorithm / termination selectors (extensions) --------------------- */
 #define PRAMAAN_ALGO_REFERENCE 0 /* the reference iteration, step sizes and restart rule */
+#define PRAMAAN_ALGO_ADAPTIVE 1  /* same iteration with Ruiz + Pock-Chambolle steps, primal
+                                    weight, averaging and KKT-based adaptive restarts */
 #define PRAMAAN_TERM_REFERENCE 0 /* abs. max primal violation, rel. max dual violation */
+#define PRAMAAN_TERM_RELATIVE_KKT 1 /* relative primal, dual residual and gap (L2, FP64) */
 
 /* LP in the reference's ModelIR form. */
 typedef struct pramaan_lp {
@@ -101,7 +104,12 @@ typedef struct pramaan_solve_result {
     int32_t restarts;          /* restarts performed                            */
     int32_t checks;            /* convergence checks performed                  */
     double solve_ms;           /* wall time inside the call                     */
-    double reserved[6];
+    double rel_primal;         /* relative KKT of the result (adaptive mode):   */
+    double rel_dual;           /*   ||primal residual||/(1+||b||), ||dual      */
+    double rel_gap;            /*   residual||/(1+||c||), |p-d|/(1+|p|+|d|)     */
+    double primal_weight;      /* final omega (adaptive mode)                   */
+    double step_size;          /* eta (adaptive mode)                           */
+    double reserved[1];
 } pramaan_solve_result;
 
 /* Library identification. */

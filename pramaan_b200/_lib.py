@@ -44,7 +44,9 @@ class CResult(C.Structure):
         ("status", i32), ("iterations", i32),
         ("primal_residual", f64), ("dual_residual", f64), ("objective_value", f64),
         ("x", P), ("row_activity", P), ("y", P),
-        ("restarts", i32), ("checks", i32), ("solve_ms", f64), ("reserved", f64 * 6),
+        ("restarts", i32), ("checks", i32), ("solve_ms", f64),
+        ("rel_primal", f64), ("rel_dual", f64), ("rel_gap", f64), ("primal_weight", f64),
+        ("step_size", f64), ("reserved", f64 * 1),
     ]
 
 

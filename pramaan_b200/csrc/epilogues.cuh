@@ -19,7 +19,7 @@ struct EpiStore {
     __device__ void init(State&) const {}
     __device__ void prefetch(int) const {}
     __device__ void apply(State&, int r, AccT v) const { y[r] = static_cast<OutT>(v); }
-    __device__ void finish(State&) const {}
+    __device__ void finish(State&, int) const {}
 };
 
 // Reference dual update with ranged-row projection
@@ -42,7 +42,7 @@ struct EpiDualRef {
         const float wp = fminf(fmaxf(w, l_r[i]), u_r[i]);
         y[i] = __fmul_rn(sig, __fsub_rn(w, wp));
     }
-    __device__ void finish(State&) const {}
+    __device__ void finish(State&, int) const {}
 };
 
 // Reference primal update with box projection and extrapolation
@@ -71,7 +71,7 @@ struct EpiPrimalRef {
         x_bar[j] = __fmaf_rn(2.0f, x_new, -x_prev);
         x[j] = x_new;
     }
-    __device__ void finish(State&) const {}
+    __device__ void finish(State&, int) const {}
 };
 
 // Reductions land in a small device array of doubles:
@@ -98,7 +98,7 @@ struct EpiRowViolRef {
         if (act < lo) s.mx = fmax(s.mx, lo - act);
         if (act > hi) s.mx = fmax(s.mx, act - hi);
     }
-    __device__ void finish(State& s) const {
+    __device__ void finish(State& s, int) const {
         block_max_to(s.mx, &slots[kSlotRowViol]);
         if (s.bad) atomic_max_nonneg(&slots[kSlotNonFinite], 1.0);
     }
@@ -135,7 +135,7 @@ struct EpiColResidRef {
         else if (at_ub && !at_lb) viol = fmax(0.0, rc);
         s.dmx = fmax(s.dmx, viol);
     }
-    __device__ void finish(State& s) const {
+    __device__ void finish(State& s, int) const {
         block_max_to(s.bmx, &slots[kSlotBoundViol]);
         block_max_to(s.dmx, &slots[kSlotDualViol]);
         if (s.bad) atomic_max_nonneg(&slots[kSlotNonFinite], 1.0);

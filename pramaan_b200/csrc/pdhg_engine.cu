@@ -17,6 +17,7 @@
 // reductions on the device (only scalars reach the host), and a check
 // interval is replayed as one CUDA graph.
 #include "pdhg_engine.cuh"
+#include "adaptive.cuh"
 
 #include <chrono>
 #include <cmath>
@@ -140,10 +141,12 @@ void validate_options(const pramaan_pdhg_options& opt) {
     if (opt.check_frequency < 1) throw InvalidArgument("pdhg options: check_frequency must be >= 1");
     if (opt.max_iterations < 0) throw InvalidArgument("pdhg options: max_iterations must be >= 0");
     if (!(opt.tolerance >= 0.0)) throw InvalidArgument("pdhg options: tolerance must be >= 0");
-    if (opt.algorithm != PRAMAAN_ALGO_REFERENCE)
+    if (opt.algorithm != PRAMAAN_ALGO_REFERENCE && opt.algorithm != PRAMAAN_ALGO_ADAPTIVE)
         throw InvalidArgument("pdhg options: unknown algorithm");
-    if (opt.termination != PRAMAAN_TERM_REFERENCE)
+    if (opt.termination != PRAMAAN_TERM_REFERENCE && opt.termination != PRAMAAN_TERM_RELATIVE_KKT)
         throw InvalidArgument("pdhg options: unknown termination criterion");
+    if (opt.algorithm == PRAMAAN_ALGO_REFERENCE && opt.termination != PRAMAAN_TERM_REFERENCE)
+        throw InvalidArgument("pdhg options: the reference algorithm uses the reference criterion");
 }
 
 PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : opt_(opt) {
@@ -210,6 +213,9 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
         PB_CUDA_CHECK(cudaGetLastError());
         PB_CUDA_CHECK(cudaMemsetAsync(y_.get(), 0, size_t(m_) * 4, st_));
     }
+    // Adaptive mode: Ruiz + Pock-Chambolle steps replace the reference steps
+    // (they also read the flat operands).
+    if (opt.algorithm == PRAMAAN_ALGO_ADAPTIVE) setup_adaptive(lp);
     // The step sizes above read the flat operands; interleave them into tile records now.
     A_.pack(st_);
     AT_.pack(st_);
@@ -226,6 +232,32 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     // tuner picks for the store-only kernel carries over to the PDHG epilogues.
     autotune_operand(A_, st_, dev_, status_.get());
     autotune_operand(AT_, st_, dev_, status_.get());
+    if (adaptive_) {
+        SpmvLauncher<EpiDualAdapt, float, float, false>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiPrimalAdapt, float, float, false>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiStoreScaled, float, float, false>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiRowKkt, double, float, true>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiRowKkt, double, float, false>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiColKkt, double, float, true>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiColKkt, double, float, false>::blocks_per_sm(dev_);
+        eta_ = 0.99 / estimate_operator_norm();
+        // initial primal weight ||C c|| / ||R b|| on the scaled problem
+        std::vector<float> hc(static_cast<size_t>(n_)), hr(static_cast<size_t>(m_));
+        if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(hc.data(), cscale_.get(), size_t(n_) * 4, cudaMemcpyDeviceToHost, st_));
+        if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(hr.data(), rscale_.get(), size_t(m_) * 4, cudaMemcpyDeviceToHost, st_));
+        PB_CUDA_CHECK(cudaStreamSynchronize(st_));
+        const double sgn = lp.obj_sense == PRAMAAN_MAXIMIZE ? -1.0 : 1.0;
+        double cs = 0.0, bs = 0.0;
+        for (int j = 0; j < n_; ++j) { const double v = sgn * lp.obj_coeffs[j] * hc[j]; cs += v * v; }
+        for (int i = 0; i < m_; ++i) {
+            const double lo = lp.row_lower[i], hi = lp.row_upper[i];
+            if (lo > -1e29) bs += (lo * hr[i]) * (lo * hr[i]);
+            if (hi < 1e29 && !(lo > -1e29 && lo == hi)) bs += (hi * hr[i]) * (hi * hr[i]);
+        }
+        cs = std::sqrt(cs);
+        bs = std::sqrt(bs);
+        set_weight(cs > 1e-10 && bs > 1e-10 ? cs / bs : 1.0);
+    }
     PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // c64 is freed on return
 }
 
@@ -236,11 +268,18 @@ PdhgEngine::~PdhgEngine() {
     for (auto& e : ev_pool_) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
     if (h_slots_) cudaFreeHost(h_slots_);
     if (h_status_) cudaFreeHost(h_status_);
+    if (h_red_) cudaFreeHost(h_red_);
     if (st_) cudaStreamDestroy(st_);
 }
 
 void PdhgEngine::launch_dual() {
     if (m_ <= 0) return;
+    if (adaptive_) {
+        EpiDualAdapt epi{sigma_.get(), lr_.get(), ur_.get(), y_.get(), ysum_.get(), scal_.get()};
+        SpmvLauncher<EpiDualAdapt, float, float, false>::launch(A_.view(false), xbar_.get(), epi,
+                                                                status_.get(), st_, dev_);
+        return;
+    }
     EpiDualRef epi{sigma_.get(), lr_.get(), ur_.get(), y_.get()};
     SpmvLauncher<EpiDualRef, float, float, false>::launch(A_.view(false), xbar_.get(), epi,
                                                           status_.get(), st_, dev_);
@@ -248,6 +287,13 @@ void PdhgEngine::launch_dual() {
 
 void PdhgEngine::launch_primal() {
     if (n_ <= 0) return;
+    if (adaptive_) {
+        EpiPrimalAdapt epi{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(),
+                           xsum_.get(), scal_.get()};
+        SpmvLauncher<EpiPrimalAdapt, float, float, false>::launch(AT_.view(false), y_.get(), epi,
+                                                                  status_.get(), st_, dev_);
+        return;
+    }
     EpiPrimalRef epi{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get()};
     SpmvLauncher<EpiPrimalRef, float, float, false>::launch(AT_.view(false), y_.get(), epi,
                                                             status_.get(), st_, dev_);
@@ -397,6 +443,9 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
     res->iterations = 0;
     res->restarts = 0;
     res->checks = 0;
+    res->rel_primal = res->rel_dual = res->rel_gap = std::numeric_limits<double>::quiet_NaN();
+    res->primal_weight = 1.0;
+    res->step_size = 1.0;
 
     const int max_it = opt_.max_iterations;
     const int cf = opt_.check_frequency;
@@ -407,7 +456,12 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
     constexpr int kMaxRestarts = 10;
     bool numerical_failure = false;
 
-    int iter = 0;
+    int iter = adaptive_ ? max_it : 0;   // the adaptive loop lives in solve_adaptive
+    if (adaptive_) {
+        solve_adaptive(lp, res);
+        restarts = res->restarts;
+        numerical_failure = res->status == PRAMAAN_STATUS_NUMERICAL_FAILURE;
+    }
     while (iter < max_it) {
         const int chunk = std::min(cf - (iter % cf), max_it - iter);
         iterate(chunk);

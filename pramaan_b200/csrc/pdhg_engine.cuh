@@ -52,6 +52,19 @@ public:
     double bytes_primal() const;
     void synchronize();
 
+    // ---- adaptive mode (pdhg_adaptive.cu) ----
+    struct Kkt {
+        double rel_p = 0, rel_d = 0, rel_gap = 0;   // PDLP relative KKT components
+        double pr2 = 0, dr2 = 0, pobj = 0, dobj = 0;  // raw sums
+        bool nonfinite = false;
+        double weighted(double omega) const;          // restart metric
+        bool converged(double tol) const { return rel_p <= tol && rel_d <= tol && rel_gap <= tol; }
+    };
+    // Relative KKT of the current iterate and of the average (synchronises).
+    void kkt_pair(Kkt& cur, Kkt& avg);
+    double primal_weight() const { return omega_; }
+    double step_size() const { return eta_; }
+
 private:
     void iterate_once();
     void launch_dual();
@@ -59,12 +72,22 @@ private:
     void check_device_status();
     void build_graph(int k);
     void drain_events();
+    // adaptive mode
+    void setup_adaptive(const pramaan_lp& lp);
+    void preconditioned_steps();
+    double estimate_operator_norm();
+    void set_weight(double omega);
+    void materialize_average();
+    void restart_to(bool average);
+    void solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res);
+    double dist2(const float* a, const float* b, const float* scale, int len);
 
     int dev_ = 0;
     cudaStream_t st_ = nullptr;
     pramaan_pdhg_options opt_{};
     int m_ = 0, n_ = 0;
     double c_norm_ = 1.0;
+    bool adaptive_ = false;
 
     CsrDevice A_, AT_;
     DevBuf<float> c_, lr_, ur_, lx_, ux_, sigma_, tau_, x_, y_, xbar_;
@@ -72,6 +95,14 @@ private:
     DevBuf<int> status_;
     double* h_slots_ = nullptr;   // pinned
     int* h_status_ = nullptr;     // pinned
+
+    // adaptive-mode state
+    DevBuf<double> cmin64_, xsum_, ysum_, part_, red_;
+    DevBuf<float> rscale_, cscale_, xa_, ya_, xl_, yl_, scal_;
+    double* h_red_ = nullptr;     // pinned, kPartSlots
+    double eta_ = 1.0, omega_ = 1.0;
+    double b_norm_ = 0.0, c_norm2_ = 0.0;
+    long long avg_count_ = 0;
 
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;

@@ -115,7 +115,8 @@ struct SpmvSmemLayout {
 //     __device__ void init(State&) const;
 //     __device__ void prefetch(int row) const;             // L2 prefetch of row data
 //     __device__ void apply(State&, int row, AccT value) const;   // row complete
-//     __device__ void finish(State&) const;                // once by every thread at exit
+//     __device__ void finish(State&, int channel) const;   // once by every thread at exit
+//                                                          // (channel 0: main kernel, 1: fixup)
 //   };
 
 __device__ __forceinline__ void prefetch_l2(const void* p) {
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
         }
         __syncwarp();
     }
-    epi.finish(est);
+    epi.finish(est, 0);
 }
 
 // Finishes the rows that cross tiles (their pieces added in tile order) and
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(256)
             epi.apply(est, A.empty_rows[k - A.num_cross], AccT(0));
         }
     }
-    epi.finish(est);
+    epi.finish(est, 1);
 }
 
 // ---------------------------------------------------------------------------

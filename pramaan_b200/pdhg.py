@@ -17,6 +17,10 @@ from . import _lib as L
 
 kInfinity = 1.0e30   # include/pramaan/ir.hpp:47
 
+# PdhgOptions.algorithm / .termination values (include/pramaan_b200.h)
+ALGO_REFERENCE, ALGO_ADAPTIVE = 0, 1
+TERM_REFERENCE, TERM_RELATIVE_KKT = 0, 1
+
 
 class ObjSense(enum.IntEnum):
     kMinimize = 0
@@ -152,6 +156,11 @@ class SolveResult:
     restarts: int = 0
     checks: int = 0
     solve_ms: float = 0.0
+    rel_primal: float = float("nan")
+    rel_dual: float = float("nan")
+    rel_gap: float = float("nan")
+    primal_weight: float = 1.0
+    step_size: float = 1.0
 
 
 class PdhgSolver:
@@ -188,6 +197,8 @@ class PdhgSolver:
         res.objective_value = cr.objective_value
         res.x, res.row_activity, res.y = x, act, y
         res.restarts, res.checks, res.solve_ms = cr.restarts, cr.checks, cr.solve_ms
+        res.rel_primal, res.rel_dual, res.rel_gap = cr.rel_primal, cr.rel_dual, cr.rel_gap
+        res.primal_weight, res.step_size = cr.primal_weight, cr.step_size
         return res
 
 
