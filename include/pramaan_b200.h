@@ -87,7 +87,12 @@ typedef struct pramaan_pdhg_options {
     int32_t device;           /* CUDA device ordinal, default 0                */
     int32_t use_graph;        /* 1: replay each check interval as a CUDA graph */
     int32_t profile_kernels;  /* 1: time every product kernel with CUDA events */
-    int32_t reserved[7];
+    int32_t refine_rounds;    /* 0: off.  Adaptive mode: up to this many FP64
+                                 iterative-refinement rounds after the FP32
+                                 solve, each re-solving the scaled correction LP
+                                 in FP32 to `tolerance`                         */
+    double refine_tolerance;  /* relative-KKT target of the refined FP64 answer */
+    int32_t reserved[6];
 } pramaan_pdhg_options;
 
 /* Result, mirroring pramaan::SolveResult (include/pramaan/simplex.hpp:40-76).

@@ -138,6 +138,8 @@ pramaan_pdhg_options defaults() {
     o.device = 0;
     o.use_graph = 1;
     o.profile_kernels = 0;
+    o.refine_rounds = 0;
+    o.refine_tolerance = 1e-8;
     return o;
 }
 

@@ -116,10 +116,11 @@ struct EpiPrimalAdapt {
 // multiplier): squared distance of (A x)_i to [row_lower, row_upper], the
 // dual objective's row terms, and the squared dual infeasibility of a
 // multiplier sign that pairs with an infinite row bound.
-struct EpiRowKkt {
+template <typename YT>
+struct EpiRowKktT {
     const double* __restrict__ row_lo;
     const double* __restrict__ row_hi;
-    const float* __restrict__ y;
+    const YT* __restrict__ y;
     double* __restrict__ part;
     int slot0;
     struct State { double pr2, dr2, dobj, bad; };
@@ -146,11 +147,12 @@ struct EpiRowKkt {
 // Column part: reduced cost rc = c + A^T y, the dual objective's bound terms,
 // the squared dual infeasibility of an rc sign that pairs with an infinite
 // variable bound, the primal objective c^T x, and x's bound violation.
-struct EpiColKkt {
+template <typename XT>
+struct EpiColKktT {
     const double* __restrict__ c;
     const double* __restrict__ var_lo;
     const double* __restrict__ var_hi;
-    const float* __restrict__ x;
+    const XT* __restrict__ x;
     double* __restrict__ part;
     int slot0;
     struct State { double pr2, dr2, dobj, pobj; };
@@ -176,6 +178,11 @@ struct EpiColKkt {
         block_sums_to<4>(v, part, channel, slot0);
     }
 };
+
+using EpiRowKkt = EpiRowKktT<float>;     // FP32 iterates
+using EpiColKkt = EpiColKktT<float>;
+using EpiRowKkt64 = EpiRowKktT<double>;  // FP64 master iterates (refinement)
+using EpiColKkt64 = EpiColKktT<double>;
 
 // y[r] = scale[r] * value (power iteration).
 struct EpiStoreScaled {

@@ -108,8 +108,9 @@ struct EpiRowViolRef {
 // bound violation of x, and the projected reduced-cost violation with rc =
 // c + Aᵀy (c and the FP32 matrix values promoted to FP64, as the reference
 // does with h_c / h_vl), `tol` slack deciding "at bound".
-struct EpiColResidRef {
-    const float* __restrict__ x;
+template <typename XT>
+struct EpiColResidRefT {
+    const XT* __restrict__ x;
     const float* __restrict__ c;
     const double* __restrict__ var_lo;
     const double* __restrict__ var_hi;
@@ -141,5 +142,6 @@ struct EpiColResidRef {
         if (s.bad) atomic_max_nonneg(&slots[kSlotNonFinite], 1.0);
     }
 };
+using EpiColResidRef = EpiColResidRefT<float>;
 
 }  // namespace pb

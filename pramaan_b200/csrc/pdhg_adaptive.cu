@@ -184,6 +184,7 @@ void PdhgEngine::setup_adaptive(const pramaan_lp& lp) {
     if (n_) PB_CUDA_CHECK(cudaMemsetAsync(xsum_.get(), 0, xsum_.bytes(), st_));
     if (m_) PB_CUDA_CHECK(cudaMemsetAsync(ysum_.get(), 0, ysum_.bytes(), st_));
     preconditioned_steps();   // replaces the reference steps in tau_ / sigma_
+    use_original_problem();
 }
 
 // Ruiz + Pock-Chambolle steps (flat operands: called before pack()).
@@ -294,6 +295,30 @@ void PdhgEngine::restart_to(bool average) {
     avg_count_ = 0;
 }
 
+namespace {
+void fill_kkt(const double* r, double b_norm, double c_norm, PdhgEngine::Kkt& q) {
+    q.pr2 = r[0] + r[4];
+    q.dr2 = r[1] + r[5];
+    q.dobj = r[2] + r[6];
+    q.pobj = r[7];
+    q.nonfinite = r[3] > 0.0 || !std::isfinite(q.pr2) || !std::isfinite(q.dr2) ||
+                  !std::isfinite(q.pobj) || !std::isfinite(q.dobj);
+    q.rel_p = std::sqrt(q.pr2) / (1.0 + b_norm);
+    q.rel_d = std::sqrt(q.dr2) / (1.0 + c_norm);
+    q.rel_gap = std::fabs(q.pobj - q.dobj) / (1.0 + std::fabs(q.pobj) + std::fabs(q.dobj));
+}
+}  // namespace
+
+void PdhgEngine::use_original_problem() {
+    pc64_ = cmin64_.get();
+    prlo_ = rlo64_.get();
+    prhi_ = rhi64_.get();
+    pvlo_ = vlo64_.get();
+    pvhi_ = vhi64_.get();
+    pb_norm_ = b_norm_;
+    pc_norm_ = c_norm2_;
+}
+
 void PdhgEngine::kkt_pair(Kkt& cur, Kkt& avg) {
     materialize_average();
     PB_CUDA_CHECK(cudaMemsetAsync(part_.get(), 0, part_.bytes(), st_));
@@ -301,14 +326,14 @@ void PdhgEngine::kkt_pair(Kkt& cur, Kkt& avg) {
     const float* ys[2] = {y_.get(), ya_.get()};
     for (int k = 0; k < 2; ++k) {
         if (m_ > 0) {
-            EpiRowKkt er{rlo64_.get(), rhi64_.get(), ys[k], part_.get(), 8 * k};
+            EpiRowKkt er{prlo_, prhi_, ys[k], part_.get(), 8 * k};
             if (A_.has_lo)
                 SpmvLauncher<EpiRowKkt, double, float, true>::launch(A_.view(true), xs[k], er, status_.get(), st_, dev_);
             else
                 SpmvLauncher<EpiRowKkt, double, float, false>::launch(A_.view(false), xs[k], er, status_.get(), st_, dev_);
         }
         if (n_ > 0) {
-            EpiColKkt ec{cmin64_.get(), vlo64_.get(), vhi64_.get(), xs[k], part_.get(), 8 * k + 4};
+            EpiColKkt ec{pc64_, pvlo_, pvhi_, xs[k], part_.get(), 8 * k + 4};
             if (AT_.has_lo)
                 SpmvLauncher<EpiColKkt, double, float, true>::launch(AT_.view(true), ys[k], ec, status_.get(), st_, dev_);
             else
@@ -319,29 +344,38 @@ void PdhgEngine::kkt_pair(Kkt& cur, Kkt& avg) {
     PB_CUDA_CHECK(cudaGetLastError());
     PB_CUDA_CHECK(cudaMemcpyAsync(h_red_, red_.get(), 16 * 8, cudaMemcpyDeviceToHost, st_));
     check_device_status();   // synchronises
-    Kkt* out[2] = {&cur, &avg};
-    for (int k = 0; k < 2; ++k) {
-        const double* r = h_red_ + 8 * k;
-        Kkt& q = *out[k];
-        q.pr2 = r[0] + r[4];
-        q.dr2 = r[1] + r[5];
-        q.dobj = r[2] + r[6];
-        q.pobj = r[7];
-        q.nonfinite = r[3] > 0.0 || !std::isfinite(q.pr2) || !std::isfinite(q.dr2) ||
-                      !std::isfinite(q.pobj) || !std::isfinite(q.dobj);
-        q.rel_p = std::sqrt(q.pr2) / (1.0 + b_norm_);
-        q.rel_d = std::sqrt(q.dr2) / (1.0 + c_norm2_);
-        q.rel_gap = std::fabs(q.pobj - q.dobj) / (1.0 + std::fabs(q.pobj) + std::fabs(q.dobj));
-    }
+    fill_kkt(h_red_, pb_norm_, pc_norm_, cur);
+    fill_kkt(h_red_ + 8, pb_norm_, pc_norm_, avg);
 }
 
-void PdhgEngine::solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res) {
-    (void)lp;
+void PdhgEngine::kkt_master(Kkt& k) {
+    PB_CUDA_CHECK(cudaMemsetAsync(part_.get(), 0, part_.bytes(), st_));
+    if (m_ > 0) {
+        EpiRowKkt64 er{rlo64_.get(), rhi64_.get(), y64_.get(), part_.get(), 0};
+        if (A_.has_lo)
+            SpmvLauncher<EpiRowKkt64, double, double, true>::launch(A_.view(true), x64_.get(), er, status_.get(), st_, dev_);
+        else
+            SpmvLauncher<EpiRowKkt64, double, double, false>::launch(A_.view(false), x64_.get(), er, status_.get(), st_, dev_);
+    }
+    if (n_ > 0) {
+        EpiColKkt64 ec{cmin64_.get(), vlo64_.get(), vhi64_.get(), x64_.get(), part_.get(), 4};
+        if (AT_.has_lo)
+            SpmvLauncher<EpiColKkt64, double, double, true>::launch(AT_.view(true), y64_.get(), ec, status_.get(), st_, dev_);
+        else
+            SpmvLauncher<EpiColKkt64, double, double, false>::launch(AT_.view(false), y64_.get(), ec, status_.get(), st_, dev_);
+    }
+    reduce_partials_kernel<<<1, 256, 0, st_>>>(part_.get(), kPartRows, 8, red_.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    PB_CUDA_CHECK(cudaMemcpyAsync(h_red_, red_.get(), 8 * 8, cudaMemcpyDeviceToHost, st_));
+    check_device_status();
+    fill_kkt(h_red_, b_norm_, c_norm2_, k);
+}
+
+int PdhgEngine::adaptive_loop(double tol, int max_it, pramaan_solve_result* res, Kkt* last_out) {
     constexpr double kSufficient = 0.2, kNecessary = 0.8, kArtificial = 0.36;
-    const int max_it = opt_.max_iterations;
     const int cf = opt_.check_frequency;
-    const double tol = opt_.tolerance;
     const bool rel_kkt = opt_.termination == PRAMAAN_TERM_RELATIVE_KKT;
+    int status = PRAMAAN_STATUS_ITERATION_LIMIT;
 
     if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(xl_.get(), x_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
     if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(yl_.get(), y_.get(), size_t(m_) * 4, cudaMemcpyDeviceToDevice, st_));
@@ -349,26 +383,25 @@ void PdhgEngine::solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res)
     kkt_pair(cur, avg);
     double kkt_restart = cur.weighted(omega_);
     double kkt_prev = std::numeric_limits<double>::infinity();
-    int last_restart = 0, restarts = 0;
-    bool failure = false;
+    int last_restart = 0;
     Kkt last = cur;
     int iter = 0;
     while (iter < max_it) {
         const int chunk = std::min(cf, max_it - iter);
         iterate(chunk);
         iter += chunk;
+        total_iterations_ += chunk;
         avg_count_ += chunk;
         kkt_pair(cur, avg);
         ++res->checks;
-        if (cur.nonfinite || avg.nonfinite) { failure = true; res->iterations = iter; break; }
+        if (cur.nonfinite || avg.nonfinite) { status = PRAMAAN_STATUS_NUMERICAL_FAILURE; break; }
         last = cur;
         if (rel_kkt) {
-            if (cur.converged(tol)) { res->status = PRAMAAN_STATUS_OPTIMAL; res->iterations = iter; break; }
+            if (cur.converged(tol)) { status = PRAMAAN_STATUS_OPTIMAL; break; }
             if (avg.converged(tol)) {
                 restart_to(true);
                 last = avg;
-                res->status = PRAMAAN_STATUS_OPTIMAL;
-                res->iterations = iter;
+                status = PRAMAAN_STATUS_OPTIMAL;
                 break;
             }
         } else {
@@ -377,8 +410,8 @@ void PdhgEngine::solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res)
             residuals(pv, dv, nf);
             res->primal_residual = pv;
             res->dual_residual = dv;
-            if (nf) { failure = true; res->iterations = iter; break; }
-            if (pv <= tol && dv <= tol) { res->status = PRAMAAN_STATUS_OPTIMAL; res->iterations = iter; break; }
+            if (nf) { status = PRAMAAN_STATUS_NUMERICAL_FAILURE; break; }
+            if (pv <= tol && dv <= tol) { status = PRAMAAN_STATUS_OPTIMAL; break; }
         }
         // ---- adaptive restart ----
         const double kc = cur.weighted(omega_), ka = avg.weighted(omega_);
@@ -401,15 +434,25 @@ void PdhgEngine::solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res)
             kkt_restart = kcand;
             kkt_prev = std::numeric_limits<double>::infinity();
             last_restart = iter;
-            ++restarts;
+            ++res->restarts;
         }
     }
-    res->restarts = restarts;
-    if (failure) res->status = PRAMAAN_STATUS_NUMERICAL_FAILURE;
-    if (res->status == PRAMAAN_STATUS_ITERATION_LIMIT) res->iterations = max_it;
+    if (last_out) *last_out = last;
+    return status;
+}
+
+void PdhgEngine::solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res) {
+    (void)lp;
+    use_original_problem();
+    total_iterations_ = 0;
+    Kkt last;
+    const int status = adaptive_loop(opt_.tolerance, opt_.max_iterations, res, &last);
+    res->status = status;
+    res->iterations = status == PRAMAAN_STATUS_ITERATION_LIMIT ? opt_.max_iterations : total_iterations_;
     res->rel_primal = last.rel_p;
     res->rel_dual = last.rel_d;
     res->rel_gap = last.rel_gap;
+    if (opt_.refine_rounds > 0 && status != PRAMAAN_STATUS_NUMERICAL_FAILURE) refine(res);
     res->primal_weight = omega_;
     res->step_size = eta_;
 }

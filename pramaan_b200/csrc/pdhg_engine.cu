@@ -499,36 +499,81 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
     {
         double pv = 0, dv = 0;
         bool nonfinite = false;
-        residuals(pv, dv, nonfinite);
+        if (refined_) reference_residuals64(pv, dv, nonfinite);
+        else residuals(pv, dv, nonfinite);
         res->primal_residual = pv;
         res->dual_residual = dv;
         if (nonfinite && res->status == PRAMAAN_STATUS_OPTIMAL)
             res->status = PRAMAAN_STATUS_NUMERICAL_FAILURE;
     }
-    std::vector<float> hx(static_cast<size_t>(n_)), hy(static_cast<size_t>(m_));
-    get_iterates(hx.data(), hy.data());
+    std::vector<double> hx(static_cast<size_t>(n_)), hy(static_cast<size_t>(m_));
+    if (refined_) {
+        // the FP64 master iterate is the answer
+        if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(hx.data(), x64_.get(), size_t(n_) * 8, cudaMemcpyDeviceToHost, st_));
+        if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(hy.data(), y64_.get(), size_t(m_) * 8, cudaMemcpyDeviceToHost, st_));
+        synchronize();
+    } else {
+        std::vector<float> fx(static_cast<size_t>(n_)), fy(static_cast<size_t>(m_));
+        get_iterates(fx.data(), fy.data());
+        for (int j = 0; j < n_; ++j) hx[j] = static_cast<double>(fx[j]);
+        for (int i = 0; i < m_; ++i) hy[i] = static_cast<double>(fy[i]);
+    }
     double obj = lp.obj_offset;
     for (int j = 0; j < n_; ++j) {
-        const double xj = static_cast<double>(hx[j]);
-        if (res->x) res->x[j] = xj;
-        obj += lp.obj_coeffs[j] * xj;
+        if (res->x) res->x[j] = hx[j];
+        obj += lp.obj_coeffs[j] * hx[j];
     }
     res->objective_value = obj;
     if (res->y)
-        for (int i = 0; i < m_; ++i) res->y[i] = static_cast<double>(hy[i]);
+        for (int i = 0; i < m_; ++i) res->y[i] = hy[i];
     if (res->row_activity && m_ > 0) {
         DevBuf<double> act{size_t(m_)};
         EpiStore<double, double> epi{act.get()};
-        if (A_.has_lo)
+        if (refined_) {
+            if (A_.has_lo)
+                SpmvLauncher<EpiStore<double, double>, double, double, true>::launch(
+                    A_.view(true), x64_.get(), epi, status_.get(), st_, dev_);
+            else
+                SpmvLauncher<EpiStore<double, double>, double, double, false>::launch(
+                    A_.view(false), x64_.get(), epi, status_.get(), st_, dev_);
+        } else if (A_.has_lo) {
             SpmvLauncher<EpiStore<double, double>, double, float, true>::launch(
                 A_.view(true), x_.get(), epi, status_.get(), st_, dev_);
-        else
+        } else {
             SpmvLauncher<EpiStore<double, double>, double, float, false>::launch(
                 A_.view(false), x_.get(), epi, status_.get(), st_, dev_);
+        }
         PB_CUDA_CHECK(cudaMemcpyAsync(res->row_activity, act.get(), size_t(m_) * 8,
                                       cudaMemcpyDeviceToHost, st_));
         synchronize();
     }
+}
+
+// Reference criterion (src/gpu/pdhg_solver.cu:107-161) evaluated on the FP64
+// master iterate of a refined solve.
+void PdhgEngine::reference_residuals64(double& pv, double& dv, bool& nonfinite) {
+    PB_CUDA_CHECK(cudaMemsetAsync(slots_.get(), 0, sizeof(double) * kSlotCount, st_));
+    if (m_ > 0) {
+        EpiRowViolRef epi{rlo64_.get(), rhi64_.get(), slots_.get()};
+        if (A_.has_lo)
+            SpmvLauncher<EpiRowViolRef, double, double, true>::launch(A_.view(true), x64_.get(), epi,
+                                                                      status_.get(), st_, dev_);
+        else
+            SpmvLauncher<EpiRowViolRef, double, double, false>::launch(A_.view(false), x64_.get(), epi,
+                                                                       status_.get(), st_, dev_);
+    }
+    if (n_ > 0) {
+        EpiColResidRefT<double> epi{x64_.get(), c_.get(), vlo64_.get(), vhi64_.get(), opt_.tolerance,
+                                    slots_.get()};
+        SpmvLauncher<EpiColResidRefT<double>, double, double, false>::launch(AT_.view(false), y64_.get(), epi,
+                                                                             status_.get(), st_, dev_);
+    }
+    PB_CUDA_CHECK(cudaMemcpyAsync(h_slots_, slots_.get(), sizeof(double) * kSlotCount,
+                                  cudaMemcpyDeviceToHost, st_));
+    check_device_status();
+    pv = std::max(h_slots_[kSlotRowViol], h_slots_[kSlotBoundViol]);
+    dv = h_slots_[kSlotDualViol] / c_norm_;
+    nonfinite = h_slots_[kSlotNonFinite] > 0.0;
 }
 
 }  // namespace pb

@@ -60,8 +60,11 @@ public:
         double weighted(double omega) const;          // restart metric
         bool converged(double tol) const { return rel_p <= tol && rel_d <= tol && rel_gap <= tol; }
     };
-    // Relative KKT of the current iterate and of the average (synchronises).
+    // Relative KKT of the current iterate and of the average (synchronises),
+    // for the problem the FP32 iteration currently solves.
     void kkt_pair(Kkt& cur, Kkt& avg);
+    // Relative KKT of the FP64 master iterate on the original problem.
+    void kkt_master(Kkt& k);
     double primal_weight() const { return omega_; }
     double step_size() const { return eta_; }
 
@@ -79,8 +82,15 @@ private:
     void set_weight(double omega);
     void materialize_average();
     void restart_to(bool average);
+    // Runs the adaptive loop on the current problem to `tol` within `max_it`
+    // iterations; returns the PRAMAAN_STATUS_* of the loop.
+    int adaptive_loop(double tol, int max_it, pramaan_solve_result* res, Kkt* last_out);
     void solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res);
     double dist2(const float* a, const float* b, const float* scale, int len);
+    // FP64 iterative refinement (pdhg_refine.cu)
+    void refine(pramaan_solve_result* res);
+    void use_original_problem();
+    void reference_residuals64(double& pv, double& dv, bool& nonfinite);
 
     int dev_ = 0;
     cudaStream_t st_ = nullptr;
@@ -103,6 +113,18 @@ private:
     double eta_ = 1.0, omega_ = 1.0;
     double b_norm_ = 0.0, c_norm2_ = 0.0;
     long long avg_count_ = 0;
+    // The problem the FP32 iteration solves: the original LP, or during FP64
+    // refinement the scaled correction LP (same matrix, new vectors).
+    const double* pc64_ = nullptr;
+    const double* prlo_ = nullptr;
+    const double* prhi_ = nullptr;
+    const double* pvlo_ = nullptr;
+    const double* pvhi_ = nullptr;
+    double pb_norm_ = 0.0, pc_norm_ = 0.0;
+    // FP64 refinement state
+    bool refined_ = false;
+    DevBuf<double> x64_, y64_, act64_, aty64_, cc64_, crlo64_, crhi64_, cvlo64_, cvhi64_;
+    int total_iterations_ = 0;
 
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;

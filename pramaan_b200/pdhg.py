@@ -127,6 +127,8 @@ class PdhgOptions:
     device: int = 0
     use_graph: bool = True
     profile_kernels: bool = False
+    refine_rounds: int = 0        # FP64 iterative-refinement rounds (adaptive mode)
+    refine_tolerance: float = 1e-8
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -139,6 +141,8 @@ class PdhgOptions:
         o.device = int(self.device)
         o.use_graph = int(bool(self.use_graph))
         o.profile_kernels = int(bool(self.profile_kernels))
+        o.refine_rounds = int(self.refine_rounds)
+        o.refine_tolerance = float(self.refine_tolerance)
         return o
 
 

@@ -42,7 +42,8 @@ def test_ctypes_binding_covers_header():
 def test_struct_layouts_match_header():
     # pramaan_lp: 4 int32 + double + 8 pointers; options 64 bytes; result.
     assert C.sizeof(L.CLp) == 4 * 4 + 8 + 8 * 8
-    assert C.sizeof(L.COptions) == 8 + 4 * 7 + 4 * 7
+    assert C.sizeof(L.COptions) == 8 + 4 * 8 + 8 + 4 * 6
+    assert L.COptions.refine_tolerance.offset == 40
     assert L.CResult.restarts.offset == 8 + 3 * 8 + 3 * 8
 
 
