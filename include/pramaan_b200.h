@@ -54,7 +54,8 @@ extern "C" {
 /* ---- algorithm / termination selectors (extensions) --------------------- */
 #define PRAMAAN_ALGO_REFERENCE 0 /* the reference iteration, step sizes and restart rule */
 #define PRAMAAN_ALGO_ADAPTIVE 1  /* same iteration with Ruiz + Pock-Chambolle steps, primal
-                                    weight, averaging and KKT-based adaptive restarts */
+                                    weight, averaging and KKT-based adaptive restarts;
+                                    needs PRAMAAN_TERM_RELATIVE_KKT */
 #define PRAMAAN_TERM_REFERENCE 0 /* abs. max primal violation, rel. max dual violation */
 #define PRAMAAN_TERM_RELATIVE_KKT 1 /* relative primal, dual residual and gap (L2, FP64) */
 
@@ -87,11 +88,13 @@ typedef struct pramaan_pdhg_options {
     int32_t device;           /* CUDA device ordinal, default 0                */
     int32_t use_graph;        /* 1: replay each check interval as a CUDA graph */
     int32_t profile_kernels;  /* 1: time every product kernel with CUDA events */
-    int32_t refine_rounds;    /* 0: off.  Adaptive mode: up to this many FP64
-                                 iterative-refinement rounds after the FP32
-                                 solve, each re-solving the scaled correction LP
-                                 in FP32 to `tolerance`                         */
-    double refine_tolerance;  /* relative-KKT target of the refined FP64 answer */
+    int32_t refine;           /* adaptive mode, 1 (default): FP64 master iterates
+                                 on the device, the FP32 iteration runs on the
+                                 correction and is folded into them at every
+                                 restart (iterative refinement), so tolerances
+                                 to about 1e-10 are reachable; 0: plain FP32
+                                 iterates (resolution about 1e-6)               */
+    double reserved_d;
     int32_t reserved[6];
 } pramaan_pdhg_options;
 
@@ -178,7 +181,8 @@ PRAMAAN_API int pramaan_spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_
 
 typedef struct pramaan_pdhg_session pramaan_pdhg_session;
 
-/* Uploads the LP and prepares the iteration (step sizes, transpose, x0). */
+/* Uploads the LP and prepares the reference iteration (step sizes, transpose,
+ * x0).  opt->algorithm must be PRAMAAN_ALGO_REFERENCE. */
 PRAMAAN_API int pramaan_session_create(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
                            pramaan_pdhg_session** out);
 PRAMAAN_API int pramaan_session_destroy(pramaan_pdhg_session* s);

@@ -63,6 +63,7 @@ def orc() -> C.CDLL:
         h = C.CDLL(str(ORC_PATH))
         sig = {
             "orc_spmv_f32": [i32, P, P, P, P, P],
+            "orc_spmv_f32_fma": [i32, P, P, P, P, P],
             "orc_spmv_t_f32": [i32, i32, P, P, P, P, P],
             "orc_spmv_f64": [i32, P, P, P, P, P],
             "orc_transpose_f32": [i32, i32, P, P, P, P, P, P],
@@ -104,6 +105,13 @@ def lp_struct(model) -> OrcLp:
 def spmv_f32(rp, ci, v, x, m):
     y = np.zeros(m, np.float32)
     orc().orc_spmv_f32(m, ptr(rp), ptr(ci), ptr(v), ptr(x), ptr(y))
+    return y
+
+
+def spmv_f32_fma(rp, ci, v, x, m):
+    """Row sums with one fused multiply-add per entry (the reference GPU kernel's arithmetic)."""
+    y = np.zeros(m, np.float32)
+    orc().orc_spmv_f32_fma(m, ptr(rp), ptr(ci), ptr(v), ptr(x), ptr(y))
     return y
 
 

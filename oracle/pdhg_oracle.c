@@ -69,6 +69,18 @@ ORC_API void orc_spmv_f32(int32_t m, const int32_t* rp, const int32_t* ci, const
     }
 }
 
+/* The same row sums as the GPU kernel computes them: nvcc contracts
+ * `sum += values[k] * x[col_idx[k]]` (src/gpu/pdhg_kernels.cuh:32-35) into one
+ * fused multiply-add per entry, in row order. */
+ORC_API void orc_spmv_f32_fma(int32_t m, const int32_t* rp, const int32_t* ci, const float* v,
+                              const float* x, float* y) {
+    for (int32_t i = 0; i < m; ++i) {
+        float s = 0.0f;
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) s = fmaf(v[k], x[ci[k]], s);
+        y[i] = s;
+    }
+}
+
 /* y = A^T x, FP32 scatter in row order: src/gpu/pdhg_kernels.cuh:42-54 (serialised)
  * and tests/test_gpu_pdhg.cpp:158-167. */
 ORC_API void orc_spmv_t_f32(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci,
@@ -259,7 +271,7 @@ static void state_init(const orc_lp* lp, orc_state* s) {
 
 static void state_iterate(const orc_lp* lp, orc_state* s) {
     if (s->m > 0) {
-        orc_spmv_f32(s->m, lp->row_ptr, lp->col_idx, s->v32, s->xbar, s->ax);
+        orc_spmv_f32_fma(s->m, lp->row_ptr, lp->col_idx, s->v32, s->xbar, s->ax);
         orc_dual_update(s->m, s->ax, s->sigma, s->lr, s->ur, s->y);
     }
     if (s->m > 0) orc_spmv_t_f32(s->m, s->n, lp->row_ptr, lp->col_idx, s->v32, s->y, s->aty);
@@ -381,7 +393,7 @@ ORC_API void orc_certificate(const orc_lp* lp, const double* x, double* obj, dou
 
 /* ---------------------------------------------------------------------------
  * Relative KKT error in FP64 (PDLP definitions, Applegate et al. 2021):
- *   primal  ||dist(Ax, [l_r,u_r])||_2 / (1 + ||finite row bounds||_2)
+ *   primal  ||(dist(Ax, [l_r,u_r]), dist(x, [l_x,u_x]))||_2 / (1 + ||finite row bounds||_2)
  *   dual    ||rc - proj_cone(rc)||_2 / (1 + ||c||_2),  rc = c - A^T lambda
  *   gap     |p - d| / (1 + |p| + |d|)
  * with lambda = -y (the reference's y is the negated multiplier) and the
@@ -419,6 +431,11 @@ ORC_API void orc_rel_kkt(const orc_lp* lp, const double* x, const double* y, dou
         c2 += cj * cj;
         pobj += cj * x[j];
         const double lo = lp->var_lower[j], hi = lp->var_upper[j];
+        /* x outside its bounds counts as primal residual */
+        double v = 0.0;
+        if (lo > -kInf && x[j] < lo) v = lo - x[j];
+        if (hi < kInf && x[j] > hi) v = x[j] - hi;
+        rp2 += v * v;
         const double r = rc[j];
         if (r > 0) { if (lo > -kInf) dobj += r * lo; else rd2 += r * r; }
         else if (r < 0) { if (hi < kInf) dobj += r * hi; else rd2 += r * r; }

@@ -138,8 +138,8 @@ pramaan_pdhg_options defaults() {
     o.device = 0;
     o.use_graph = 1;
     o.profile_kernels = 0;
-    o.refine_rounds = 0;
-    o.refine_tolerance = 1e-8;
+    o.refine = 1;
+    o.reserved_d = 0.0;
     return o;
 }
 
@@ -261,6 +261,8 @@ int pramaan_session_create(const pramaan_lp* lp, const pramaan_pdhg_options* opt
         if (!lp || !out) throw InvalidArgument("lp and out must not be NULL");
         *out = nullptr;
         const pramaan_pdhg_options o = opt ? *opt : defaults();
+        if (o.algorithm != PRAMAAN_ALGO_REFERENCE)
+            throw InvalidArgument("sessions step the reference iteration (PRAMAAN_ALGO_REFERENCE)");
         DeviceGuard g(o.device);
         auto s = std::make_unique<pramaan_pdhg_session>();
         s->eng = std::make_unique<PdhgEngine>(*lp, o);

@@ -53,37 +53,58 @@ __device__ __forceinline__ void block_sums_to(const double (&v)[K], double* __re
     __syncthreads();
 }
 
-// Dual update of the reference (src/gpu/pdhg_kernels.cuh:72-89) with the
-// adaptive step sigma_i * scal[1], plus the running sum of y.
+// The adaptive iteration runs on corrections around FP64 master iterates
+// (x = x_m + d, y = y_m + e; pdhg_adaptive.cu folds d, e into the master at
+// every restart).  Everything the update needs from the master is folded
+// into FP32 vectors when the master changes:
+//   r_lo = A x_m - l_r,  r_hi = A x_m - u_r   (+-1e30 where the bound is infinite)
+//   c'   = c + A^T y_m,  l'_x = l_x - x_m,  u'_x = u_x - x_m.
+//
+// Dual update (the reference's, src/gpu/pdhg_kernels.cuh:72-89, with the
+// adaptive step s = sigma_i * scal[1]) in a form that keeps FP32 precision
+// when y/s is much larger than A x̄:
+//   w = y/s + (A x̄)_i  only decides the case;
+//   w > u_r:  y' = y + s ((A x̄)_i - u_r)    w < l_r:  y' = y + s ((A x̄)_i - l_r)
+//   else:     y' = 0
+// which is s (w - clamp(w, l_r, u_r)) rearranged.  In correction form
+// (A x̄ = A x_m + A d̄, y = y_m + e) the residual differences come straight
+// from r_lo / r_hi and the inactive case is e' = -y_m.  Adds e' to the
+// running FP64 sum of the epoch's average.
 struct EpiDualAdapt {
     const float* __restrict__ sigma;
-    const float* __restrict__ l_r;
-    const float* __restrict__ u_r;
-    float* __restrict__ y;
-    double* __restrict__ ysum;
+    const float* __restrict__ r_lo;
+    const float* __restrict__ r_hi;
+    const float* __restrict__ y_m;   // FP32 copy of the master dual
+    float* __restrict__ e;
+    double* __restrict__ esum;
     const float* __restrict__ scal;
     using State = NoState;
     __device__ void init(State&) const {}
     __device__ void prefetch(int i) const {
-        prefetch_l2(sigma + i); prefetch_l2(l_r + i); prefetch_l2(u_r + i); prefetch_l2(y + i);
-        prefetch_l2(ysum + i);
+        prefetch_l2(sigma + i); prefetch_l2(r_lo + i); prefetch_l2(r_hi + i); prefetch_l2(y_m + i);
+        prefetch_l2(e + i); prefetch_l2(esum + i);
     }
-    __device__ void apply(State&, int i, float ax) const {
-        const float sig = __fmul_rn(sigma[i], scal[1]);
-        float yn = y[i];
-        if (sig > 0.0f) {
-            const float w = __fadd_rn(__fdiv_rn(yn, sig), ax);
-            const float wp = fminf(fmaxf(w, l_r[i]), u_r[i]);
-            yn = __fmul_rn(sig, __fsub_rn(w, wp));
+    __device__ void apply(State&, int i, float ad) const {
+        const float s = __fmul_rn(sigma[i], scal[1]);
+        float en = e[i];
+        if (s > 0.0f) {
+            const float ym = y_m[i];
+            const float q = __fdiv_rn(__fadd_rn(ym, en), s);
+            const float hi = __fadd_rn(ad, r_hi[i]);   // (A x̄)_i - u_r
+            const float lo = __fadd_rn(ad, r_lo[i]);   // (A x̄)_i - l_r
+            if (__fadd_rn(q, hi) > 0.0f) en = __fmaf_rn(s, hi, en);
+            else if (__fadd_rn(q, lo) < 0.0f) en = __fmaf_rn(s, lo, en);
+            else en = -ym;
         }
-        y[i] = yn;
-        ysum[i] += static_cast<double>(yn);
+        e[i] = en;
+        esum[i] += static_cast<double>(en);
     }
     __device__ void finish(State&, int) const {}
 };
 
 // Primal update of the reference (src/gpu/pdhg_kernels.cuh:95-109) with the
-// adaptive step tau_j * scal[0], plus the running sum of x.
+// adaptive step tau_j * scal[0], plus the running sum of x.  On corrections
+// the same formula applies to d with c' and the shifted bounds l'_x, u'_x.
 struct EpiPrimalAdapt {
     const float* __restrict__ tau;
     const float* __restrict__ c;
@@ -113,28 +134,35 @@ struct EpiPrimalAdapt {
 
 // Row part of the relative KKT error (FP64, on the original problem in
 // minimisation form; lambda = -y since y is the reference's negated
-// multiplier): squared distance of (A x)_i to [row_lower, row_upper], the
-// dual objective's row terms, and the squared dual infeasibility of a
-// multiplier sign that pairs with an infinite row bound.
-template <typename YT>
-struct EpiRowKktT {
+// multiplier) of x = x_m + d, y = y_m + e: the SpMV delivers (A d)_i, the
+// master's activity A x_m is added in FP64.  Sums the squared distance of
+// (A x)_i to [row_lower, row_upper], the dual objective's row terms, and the
+// squared dual infeasibility of a multiplier sign that pairs with an
+// infinite row bound.
+struct EpiRowKkt {
     const double* __restrict__ row_lo;
     const double* __restrict__ row_hi;
-    const YT* __restrict__ y;
+    const double* __restrict__ act_m;   // A x_m
+    const double* __restrict__ y_m;
+    const float* __restrict__ e;
     double* __restrict__ part;
     int slot0;
     struct State { double pr2, dr2, dobj, bad; };
     __device__ void init(State& s) const { s.pr2 = s.dr2 = s.dobj = s.bad = 0.0; }
-    __device__ void prefetch(int i) const { prefetch_l2(row_lo + i); prefetch_l2(row_hi + i); prefetch_l2(y + i); }
-    __device__ void apply(State& s, int i, double act) const {
+    __device__ void prefetch(int i) const {
+        prefetch_l2(row_lo + i); prefetch_l2(row_hi + i); prefetch_l2(act_m + i); prefetch_l2(y_m + i);
+        prefetch_l2(e + i);
+    }
+    __device__ void apply(State& s, int i, double ad) const {
         const double lo = row_lo[i], hi = row_hi[i];
+        const double act = act_m[i] + ad;
         if (!isfinite(act)) { s.bad = 1.0; return; }
         const bool lo_f = lo > -1e29, hi_f = hi < 1e29;
         double d = 0.0;
         if (lo_f && act < lo) d = lo - act;
         if (hi_f && act > hi) d = act - hi;
         s.pr2 += d * d;
-        const double lam = -static_cast<double>(y[i]);
+        const double lam = -(y_m[i] + static_cast<double>(e[i]));
         if (lam > 0.0) { if (lo_f) s.dobj += lam * lo; else s.dr2 += lam * lam; }
         else if (lam < 0.0) { if (hi_f) s.dobj += lam * hi; else s.dr2 += lam * lam; }
     }
@@ -144,45 +172,44 @@ struct EpiRowKktT {
     }
 };
 
-// Column part: reduced cost rc = c + A^T y, the dual objective's bound terms,
-// the squared dual infeasibility of an rc sign that pairs with an infinite
-// variable bound, the primal objective c^T x, and x's bound violation.
-template <typename XT>
-struct EpiColKktT {
+// Column part: reduced cost rc = c + A^T y = rc_m + (A^T e)_j with the
+// master's rc_m = c + A^T y_m in FP64, the dual objective's bound terms, the
+// squared dual infeasibility of an rc sign that pairs with an infinite
+// variable bound, the primal objective c^T x, and x's bound violation
+// (x = x_m + d; FP32 rounding can leave it just outside an FP64 bound).
+struct EpiColKkt {
     const double* __restrict__ c;
     const double* __restrict__ var_lo;
     const double* __restrict__ var_hi;
-    const XT* __restrict__ x;
+    const double* __restrict__ rc_m;
+    const double* __restrict__ x_m;
+    const float* __restrict__ d;
     double* __restrict__ part;
     int slot0;
     struct State { double pr2, dr2, dobj, pobj; };
     __device__ void init(State& s) const { s.pr2 = s.dr2 = s.dobj = s.pobj = 0.0; }
     __device__ void prefetch(int j) const {
-        prefetch_l2(c + j); prefetch_l2(var_lo + j); prefetch_l2(var_hi + j); prefetch_l2(x + j);
+        prefetch_l2(c + j); prefetch_l2(var_lo + j); prefetch_l2(var_hi + j); prefetch_l2(rc_m + j);
+        prefetch_l2(x_m + j); prefetch_l2(d + j);
     }
-    __device__ void apply(State& s, int j, double aty) const {
+    __device__ void apply(State& s, int j, double ate) const {
         const double lo = var_lo[j], hi = var_hi[j], cj = c[j];
-        const double xj = static_cast<double>(x[j]);
+        const double xj = x_m[j] + static_cast<double>(d[j]);
         const bool lo_f = lo > -1e29, hi_f = hi < 1e29;
-        const double rc = cj + aty;
+        const double rc = rc_m[j] + ate;
         if (rc > 0.0) { if (lo_f) s.dobj += rc * lo; else s.dr2 += rc * rc; }
         else if (rc < 0.0) { if (hi_f) s.dobj += rc * hi; else s.dr2 += rc * rc; }
         s.pobj += cj * xj;
-        double d = 0.0;
-        if (lo_f && xj < lo) d = lo - xj;
-        if (hi_f && xj > hi) d = xj - hi;
-        s.pr2 += d * d;
+        double v = 0.0;
+        if (lo_f && xj < lo) v = lo - xj;
+        if (hi_f && xj > hi) v = xj - hi;
+        s.pr2 += v * v;
     }
     __device__ void finish(State& s, int channel) const {
         const double v[4] = {s.pr2, s.dr2, s.dobj, s.pobj};
         block_sums_to<4>(v, part, channel, slot0);
     }
 };
-
-using EpiRowKkt = EpiRowKktT<float>;     // FP32 iterates
-using EpiColKkt = EpiColKktT<float>;
-using EpiRowKkt64 = EpiRowKktT<double>;  // FP64 master iterates (refinement)
-using EpiColKkt64 = EpiColKktT<double>;
 
 // y[r] = scale[r] * value (power iteration).
 struct EpiStoreScaled {

@@ -24,6 +24,28 @@
 //   * termination on the relative KKT error of the original problem in FP64:
 //     ||dist(Ax, [l_r, u_r])||/(1+||b||), ||dual infeasibility||/(1+||c||),
 //     |p - d|/(1 + |p| + |d|) all <= tolerance.
+//
+// FP64 iterative refinement (options.refine = 1, the default).  FP32
+// iterates resolve the relative KKT error only to about 1e-6 (rounding the
+// exact optimum of a small random LP to FP32 can already leave a 2e-6 gap).
+// The solver therefore keeps FP64 master iterates (x_m, y_m) on the device
+// and runs the FP32 iteration on the correction (d, e), x = x_m + d,
+// y = y_m + e.  The correction problem is the original one translated by
+// the master: its FP32 data are the FP64 residuals of the master rounded
+// once, A x_m - l_r and A x_m - u_r for the dual update, c + A^T y_m and
+// l_x - x_m, u_x - x_m for the primal update (computed by FP64 products with
+// the FP32 hi + lo split of the matrix).  At every restart the restart point
+// is folded into the master (x_m += d, y_m += e in FP64) and the residuals
+// are recomputed, so the FP32 numbers always hold the remaining correction,
+// which shrinks with the error: the FP32 resolution applies to the
+// correction, not to the answer.  In exact arithmetic the translation
+// changes nothing (PDHG commutes with it), so the iteration, the restarts
+// and omega are those of the untranslated method; the products inside the
+// iteration stay FP32 (8 bytes per non-zero).  This is iterative refinement
+// in the sense of Gleixner, Steffy and Wolter (INFORMS J. Computing 2016) —
+// FP64 residuals, a correction problem solved in lower precision, an FP64
+// update — with one restart epoch of the correction problem per round and
+// no rescaling (PDHG's restarts already contract the correction).
 #include "adaptive.cuh"
 #include "pdhg_engine.cuh"
 
@@ -84,15 +106,15 @@ __global__ void pc_step_kernel(const int* __restrict__ rp, const int* __restrict
 
 // Deterministic dot product / squared distance: per-block partials (slot
 // `slot` of the partial rows), then one block sums them in a fixed order.
-//   sub == null:   sum a_i b_i
-//   sub != null:   sum ((a_i - sub_i) / scale_i)^2   (scale may be null)
+//   b != null:             sum a_i b_i
+//   b == null:             sum ((a_i - sub_i) / scale_i)^2   (sub, scale may be null)
 __global__ void dot_partials_kernel(const float* __restrict__ a, const float* __restrict__ b,
                                     const float* __restrict__ sub, const float* __restrict__ scale,
                                     int n, double* __restrict__ part, int slot) {
     double acc = 0.0;
     PB_GRID_STRIDE(i, n) {
-        if (sub) {
-            double u = static_cast<double>(a[i]) - static_cast<double>(sub[i]);
+        if (!b) {
+            double u = static_cast<double>(a[i]) - (sub ? static_cast<double>(sub[i]) : 0.0);
             if (scale) u /= static_cast<double>(scale[i]);
             acc += u * u;
         } else {
@@ -151,6 +173,84 @@ __global__ void set_scalars_kernel(float* __restrict__ scal, float primal, float
     if (blockIdx.x == 0 && threadIdx.x == 0) { scal[0] = primal; scal[1] = dual; }
 }
 
+constexpr double kInf = 1e29;
+constexpr float kFltInf = 1e30f;
+
+// Starting master: x_m = clamp(0, l_x, u_x) (the reference's x0), y_m = 0.
+__global__ void init_master_kernel(const double* __restrict__ vlo, const double* __restrict__ vhi, int n,
+                                   double* __restrict__ xm) {
+    PB_GRID_STRIDE(j, n) {
+        double v = 0.0;
+        if (vhi[j] < kInf && v > vhi[j]) v = vhi[j];
+        if (vlo[j] > -kInf && v < vlo[j]) v = vlo[j];
+        xm[j] = v;
+    }
+}
+
+// master += correction; correction <- 0 (and the second buffer, if given).
+__global__ void fold_into_kernel(double* __restrict__ master, float* __restrict__ corr,
+                                 float* __restrict__ corr2, int n) {
+    PB_GRID_STRIDE(i, n) {
+        master[i] += static_cast<double>(corr[i]);
+        corr[i] = 0.0f;
+        if (corr2) corr2[i] = 0.0f;
+    }
+}
+
+// Row data of the correction problem: r_lo = A x_m - l_r, r_hi = A x_m - u_r
+// (+1e30 / -1e30 for an infinite bound), and the FP32 copy of y_m.
+__global__ void fold_rows_kernel(const double* __restrict__ rlo, const double* __restrict__ rhi,
+                                 const double* __restrict__ act, const double* __restrict__ ym, int m,
+                                 float* __restrict__ r_lo, float* __restrict__ r_hi, float* __restrict__ ym32) {
+    PB_GRID_STRIDE(i, m) {
+        const double a = act[i], lo = rlo[i], hi = rhi[i];
+        r_lo[i] = lo > -kInf ? static_cast<float>(a - lo) : kFltInf;
+        r_hi[i] = hi < kInf ? static_cast<float>(a - hi) : -kFltInf;
+        ym32[i] = static_cast<float>(ym[i]);
+    }
+}
+
+// Column data: rc_m = c + A^T y_m (in place over A^T y_m) and its FP32 copy
+// as the correction's cost; bounds l_x - x_m, u_x - x_m.
+__global__ void fold_cols_kernel(const double* __restrict__ c, const double* __restrict__ vlo,
+                                 const double* __restrict__ vhi, const double* __restrict__ xm, int n,
+                                 double* __restrict__ rc, float* __restrict__ c32, float* __restrict__ lx,
+                                 float* __restrict__ ux) {
+    PB_GRID_STRIDE(j, n) {
+        const double r = c[j] + rc[j];
+        rc[j] = r;
+        c32[j] = static_cast<float>(r);
+        const double lo = vlo[j], hi = vhi[j], x = xm[j];
+        lx[j] = lo > -kInf ? static_cast<float>(lo - x) : -kFltInf;
+        ux[j] = hi < kInf ? static_cast<float>(hi - x) : kFltInf;
+    }
+}
+
+// out = master + correction in FP64.
+__global__ void sum_out_kernel(const double* __restrict__ master, const float* __restrict__ corr, int n,
+                               double* __restrict__ out) {
+    PB_GRID_STRIDE(i, n) out[i] = master[i] + static_cast<double>(corr[i]);
+}
+
+// The original problem's FP32 vectors (as the reference prepares them).
+__global__ void restore_cols_kernel(const double* __restrict__ c64, const double* __restrict__ vlo,
+                                    const double* __restrict__ vhi, int n, float* __restrict__ c32,
+                                    float* __restrict__ flo, float* __restrict__ fhi) {
+    PB_GRID_STRIDE(j, n) {
+        c32[j] = static_cast<float>(c64[j]);
+        flo[j] = vlo[j] <= -kInf ? -kFltInf : static_cast<float>(vlo[j]);
+        fhi[j] = vhi[j] >= kInf ? kFltInf : static_cast<float>(vhi[j]);
+    }
+}
+
+__global__ void restore_rows_kernel(const double* __restrict__ rlo, const double* __restrict__ rhi, int m,
+                                    float* __restrict__ flo, float* __restrict__ fhi) {
+    PB_GRID_STRIDE(i, m) {
+        flo[i] = rlo[i] <= -kInf ? -kFltInf : static_cast<float>(rlo[i]);
+        fhi[i] = rhi[i] >= kInf ? kFltInf : static_cast<float>(rhi[i]);
+    }
+}
+
 }  // namespace
 
 double PdhgEngine::Kkt::weighted(double omega) const {
@@ -175,7 +275,9 @@ void PdhgEngine::setup_adaptive(const pramaan_lp& lp) {
     cmin64_.alloc(n_);
     if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(cmin64_.get(), cmin.data(), size_t(n_) * 8, cudaMemcpyHostToDevice, st_));
     xsum_.alloc(n_); ysum_.alloc(m_);
-    xa_.alloc(n_); ya_.alloc(m_); xl_.alloc(n_); yl_.alloc(m_);
+    xa_.alloc(n_); ya_.alloc(m_);
+    if (!opt_.refine) { xl_.alloc(n_); yl_.alloc(m_); }
+    xm64_.alloc(n_); ym64_.alloc(m_); actm64_.alloc(m_); rcm64_.alloc(n_); ym32_.alloc(m_);
     rscale_.alloc(m_); cscale_.alloc(n_);
     scal_.alloc(2);
     part_.alloc(size_t(kPartRows) * kPartSlots);
@@ -184,7 +286,6 @@ void PdhgEngine::setup_adaptive(const pramaan_lp& lp) {
     if (n_) PB_CUDA_CHECK(cudaMemsetAsync(xsum_.get(), 0, xsum_.bytes(), st_));
     if (m_) PB_CUDA_CHECK(cudaMemsetAsync(ysum_.get(), 0, ysum_.bytes(), st_));
     preconditioned_steps();   // replaces the reference steps in tau_ / sigma_
-    use_original_problem();
 }
 
 // Ruiz + Pock-Chambolle steps (flat operands: called before pack()).
@@ -295,6 +396,41 @@ void PdhgEngine::restart_to(bool average) {
     avg_count_ = 0;
 }
 
+void PdhgEngine::fold(bool first) {
+    if (first) {
+        if (n_) init_master_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(vlo64_.get(), vhi64_.get(), n_, xm64_.get());
+        if (m_) PB_CUDA_CHECK(cudaMemsetAsync(ym64_.get(), 0, ym64_.bytes(), st_));
+        if (n_) PB_CUDA_CHECK(cudaMemsetAsync(x_.get(), 0, size_t(n_) * 4, st_));
+        if (n_) PB_CUDA_CHECK(cudaMemsetAsync(xbar_.get(), 0, size_t(n_) * 4, st_));
+        if (m_) PB_CUDA_CHECK(cudaMemsetAsync(y_.get(), 0, size_t(m_) * 4, st_));
+    } else {
+        if (n_) fold_into_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(xm64_.get(), x_.get(), xbar_.get(), n_);
+        if (m_) fold_into_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(ym64_.get(), y_.get(), nullptr, m_);
+        ++folds_;
+    }
+    PB_CUDA_CHECK(cudaGetLastError());
+    // FP64 residuals of the master (hi + lo matrix values, FP64 accumulation)
+    if (m_) {
+        EpiStore<double, double> e{actm64_.get()};
+        if (A_.has_lo)
+            SpmvLauncher<EpiStore<double, double>, double, double, true>::launch(A_.view(true), xm64_.get(), e, status_.get(), st_, dev_);
+        else
+            SpmvLauncher<EpiStore<double, double>, double, double, false>::launch(A_.view(false), xm64_.get(), e, status_.get(), st_, dev_);
+        fold_rows_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(rlo64_.get(), rhi64_.get(), actm64_.get(), ym64_.get(), m_,
+                                                            lr_.get(), ur_.get(), ym32_.get());
+    }
+    if (n_) {
+        EpiStore<double, double> e{rcm64_.get()};
+        if (AT_.has_lo)
+            SpmvLauncher<EpiStore<double, double>, double, double, true>::launch(AT_.view(true), ym64_.get(), e, status_.get(), st_, dev_);
+        else
+            SpmvLauncher<EpiStore<double, double>, double, double, false>::launch(AT_.view(false), ym64_.get(), e, status_.get(), st_, dev_);
+        fold_cols_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(cmin64_.get(), vlo64_.get(), vhi64_.get(), xm64_.get(), n_,
+                                                            rcm64_.get(), c_.get(), lx_.get(), ux_.get());
+    }
+    PB_CUDA_CHECK(cudaGetLastError());
+}
+
 namespace {
 void fill_kkt(const double* r, double b_norm, double c_norm, PdhgEngine::Kkt& q) {
     q.pr2 = r[0] + r[4];
@@ -309,16 +445,6 @@ void fill_kkt(const double* r, double b_norm, double c_norm, PdhgEngine::Kkt& q)
 }
 }  // namespace
 
-void PdhgEngine::use_original_problem() {
-    pc64_ = cmin64_.get();
-    prlo_ = rlo64_.get();
-    prhi_ = rhi64_.get();
-    pvlo_ = vlo64_.get();
-    pvhi_ = vhi64_.get();
-    pb_norm_ = b_norm_;
-    pc_norm_ = c_norm2_;
-}
-
 void PdhgEngine::kkt_pair(Kkt& cur, Kkt& avg) {
     materialize_average();
     PB_CUDA_CHECK(cudaMemsetAsync(part_.get(), 0, part_.bytes(), st_));
@@ -326,14 +452,15 @@ void PdhgEngine::kkt_pair(Kkt& cur, Kkt& avg) {
     const float* ys[2] = {y_.get(), ya_.get()};
     for (int k = 0; k < 2; ++k) {
         if (m_ > 0) {
-            EpiRowKkt er{prlo_, prhi_, ys[k], part_.get(), 8 * k};
+            EpiRowKkt er{rlo64_.get(), rhi64_.get(), actm64_.get(), ym64_.get(), ys[k], part_.get(), 8 * k};
             if (A_.has_lo)
                 SpmvLauncher<EpiRowKkt, double, float, true>::launch(A_.view(true), xs[k], er, status_.get(), st_, dev_);
             else
                 SpmvLauncher<EpiRowKkt, double, float, false>::launch(A_.view(false), xs[k], er, status_.get(), st_, dev_);
         }
         if (n_ > 0) {
-            EpiColKkt ec{pc64_, pvlo_, pvhi_, xs[k], part_.get(), 8 * k + 4};
+            EpiColKkt ec{cmin64_.get(), vlo64_.get(), vhi64_.get(), rcm64_.get(), xm64_.get(), xs[k], part_.get(),
+                         8 * k + 4};
             if (AT_.has_lo)
                 SpmvLauncher<EpiColKkt, double, float, true>::launch(AT_.view(true), ys[k], ec, status_.get(), st_, dev_);
             else
@@ -344,41 +471,44 @@ void PdhgEngine::kkt_pair(Kkt& cur, Kkt& avg) {
     PB_CUDA_CHECK(cudaGetLastError());
     PB_CUDA_CHECK(cudaMemcpyAsync(h_red_, red_.get(), 16 * 8, cudaMemcpyDeviceToHost, st_));
     check_device_status();   // synchronises
-    fill_kkt(h_red_, pb_norm_, pc_norm_, cur);
-    fill_kkt(h_red_ + 8, pb_norm_, pc_norm_, avg);
+    fill_kkt(h_red_, b_norm_, c_norm2_, cur);
+    fill_kkt(h_red_ + 8, b_norm_, c_norm2_, avg);
 }
 
-void PdhgEngine::kkt_master(Kkt& k) {
-    PB_CUDA_CHECK(cudaMemsetAsync(part_.get(), 0, part_.bytes(), st_));
-    if (m_ > 0) {
-        EpiRowKkt64 er{rlo64_.get(), rhi64_.get(), y64_.get(), part_.get(), 0};
-        if (A_.has_lo)
-            SpmvLauncher<EpiRowKkt64, double, double, true>::launch(A_.view(true), x64_.get(), er, status_.get(), st_, dev_);
-        else
-            SpmvLauncher<EpiRowKkt64, double, double, false>::launch(A_.view(false), x64_.get(), er, status_.get(), st_, dev_);
+void PdhgEngine::finish_adaptive() {
+    x64_.alloc(n_);
+    y64_.alloc(m_);
+    if (n_) sum_out_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(xm64_.get(), x_.get(), n_, x64_.get());
+    if (m_) sum_out_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(ym64_.get(), y_.get(), m_, y64_.get());
+    // the FP32 vectors and iterates of the original problem again
+    if (n_) {
+        restore_cols_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(cmin64_.get(), vlo64_.get(), vhi64_.get(), n_,
+                                                               c_.get(), lx_.get(), ux_.get());
+        average_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(x64_.get(), n_, 1.0, x_.get());
+        PB_CUDA_CHECK(cudaMemcpyAsync(xbar_.get(), x_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
     }
-    if (n_ > 0) {
-        EpiColKkt64 ec{cmin64_.get(), vlo64_.get(), vhi64_.get(), x64_.get(), part_.get(), 4};
-        if (AT_.has_lo)
-            SpmvLauncher<EpiColKkt64, double, double, true>::launch(AT_.view(true), y64_.get(), ec, status_.get(), st_, dev_);
-        else
-            SpmvLauncher<EpiColKkt64, double, double, false>::launch(AT_.view(false), y64_.get(), ec, status_.get(), st_, dev_);
+    if (m_) {
+        restore_rows_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(rlo64_.get(), rhi64_.get(), m_, lr_.get(), ur_.get());
+        average_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(y64_.get(), m_, 1.0, y_.get());
     }
-    reduce_partials_kernel<<<1, 256, 0, st_>>>(part_.get(), kPartRows, 8, red_.get());
     PB_CUDA_CHECK(cudaGetLastError());
-    PB_CUDA_CHECK(cudaMemcpyAsync(h_red_, red_.get(), 8 * 8, cudaMemcpyDeviceToHost, st_));
-    check_device_status();
-    fill_kkt(h_red_, b_norm_, c_norm2_, k);
+    master_out_ = true;
 }
 
-int PdhgEngine::adaptive_loop(double tol, int max_it, pramaan_solve_result* res, Kkt* last_out) {
+void PdhgEngine::solve_adaptive(pramaan_solve_result* res) {
     constexpr double kSufficient = 0.2, kNecessary = 0.8, kArtificial = 0.36;
     const int cf = opt_.check_frequency;
-    const bool rel_kkt = opt_.termination == PRAMAAN_TERM_RELATIVE_KKT;
+    const int max_it = opt_.max_iterations;
+    const double tol = opt_.tolerance;
+    const bool refine = opt_.refine != 0;
     int status = PRAMAAN_STATUS_ITERATION_LIMIT;
-
-    if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(xl_.get(), x_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
-    if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(yl_.get(), y_.get(), size_t(m_) * 4, cudaMemcpyDeviceToDevice, st_));
+    folds_ = 0;
+    avg_count_ = 0;
+    fold(true);
+    if (!refine) {
+        if (n_) PB_CUDA_CHECK(cudaMemsetAsync(xl_.get(), 0, xl_.bytes(), st_));
+        if (m_) PB_CUDA_CHECK(cudaMemsetAsync(yl_.get(), 0, yl_.bytes(), st_));
+    }
     Kkt cur, avg;
     kkt_pair(cur, avg);
     double kkt_restart = cur.weighted(omega_);
@@ -386,32 +516,22 @@ int PdhgEngine::adaptive_loop(double tol, int max_it, pramaan_solve_result* res,
     int last_restart = 0;
     Kkt last = cur;
     int iter = 0;
-    while (iter < max_it) {
+    if (cur.converged(tol)) status = PRAMAAN_STATUS_OPTIMAL;
+    while (status == PRAMAAN_STATUS_ITERATION_LIMIT && iter < max_it) {
         const int chunk = std::min(cf, max_it - iter);
         iterate(chunk);
         iter += chunk;
-        total_iterations_ += chunk;
         avg_count_ += chunk;
         kkt_pair(cur, avg);
         ++res->checks;
         if (cur.nonfinite || avg.nonfinite) { status = PRAMAAN_STATUS_NUMERICAL_FAILURE; break; }
         last = cur;
-        if (rel_kkt) {
-            if (cur.converged(tol)) { status = PRAMAAN_STATUS_OPTIMAL; break; }
-            if (avg.converged(tol)) {
-                restart_to(true);
-                last = avg;
-                status = PRAMAAN_STATUS_OPTIMAL;
-                break;
-            }
-        } else {
-            double pv = 0, dv = 0;
-            bool nf = false;
-            residuals(pv, dv, nf);
-            res->primal_residual = pv;
-            res->dual_residual = dv;
-            if (nf) { status = PRAMAAN_STATUS_NUMERICAL_FAILURE; break; }
-            if (pv <= tol && dv <= tol) { status = PRAMAAN_STATUS_OPTIMAL; break; }
+        if (cur.converged(tol)) { status = PRAMAAN_STATUS_OPTIMAL; break; }
+        if (avg.converged(tol)) {
+            restart_to(true);
+            last = avg;
+            status = PRAMAAN_STATUS_OPTIMAL;
+            break;
         }
         // ---- adaptive restart ----
         const double kc = cur.weighted(omega_), ka = avg.weighted(omega_);
@@ -421,38 +541,33 @@ int PdhgEngine::adaptive_loop(double tol, int max_it, pramaan_solve_result* res,
                              (kcand <= kNecessary * kkt_restart && kcand > kkt_prev) ||
                              (iter - last_restart) >= kArtificial * iter;
         kkt_prev = kcand;
-        if (restart) {
-            restart_to(use_avg);
-            const double dx = std::sqrt(dist2(x_.get(), xl_.get(), cscale_.get(), n_));
-            const double dy = std::sqrt(dist2(y_.get(), yl_.get(), rscale_.get(), m_));
-            if (dx > 1e-10 && dy > 1e-10) {
-                const double w = std::exp(0.5 * std::log(dy / dx) + 0.5 * std::log(omega_));
-                if (std::isfinite(w) && w > 0.0) set_weight(w);
-            }
+        if (!restart) continue;
+        restart_to(use_avg);
+        // movement since the previous restart point, in the scaled norms: with
+        // refinement the master is that point, so the correction itself
+        const double dx = std::sqrt(dist2(x_.get(), refine ? nullptr : xl_.get(), cscale_.get(), n_));
+        const double dy = std::sqrt(dist2(y_.get(), refine ? nullptr : yl_.get(), rscale_.get(), m_));
+        if (dx > 1e-10 && dy > 1e-10) {
+            const double w = std::exp(0.5 * std::log(dy / dx) + 0.5 * std::log(omega_));
+            if (std::isfinite(w) && w > 0.0) set_weight(w);
+        }
+        if (refine) {
+            fold(false);
+        } else {
             if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(xl_.get(), x_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
             if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(yl_.get(), y_.get(), size_t(m_) * 4, cudaMemcpyDeviceToDevice, st_));
-            kkt_restart = kcand;
-            kkt_prev = std::numeric_limits<double>::infinity();
-            last_restart = iter;
-            ++res->restarts;
         }
+        kkt_restart = kcand;
+        kkt_prev = std::numeric_limits<double>::infinity();
+        last_restart = iter;
+        ++res->restarts;
     }
-    if (last_out) *last_out = last;
-    return status;
-}
-
-void PdhgEngine::solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res) {
-    (void)lp;
-    use_original_problem();
-    total_iterations_ = 0;
-    Kkt last;
-    const int status = adaptive_loop(opt_.tolerance, opt_.max_iterations, res, &last);
+    finish_adaptive();
     res->status = status;
-    res->iterations = status == PRAMAAN_STATUS_ITERATION_LIMIT ? opt_.max_iterations : total_iterations_;
+    res->iterations = status == PRAMAAN_STATUS_ITERATION_LIMIT ? max_it : iter;
     res->rel_primal = last.rel_p;
     res->rel_dual = last.rel_d;
     res->rel_gap = last.rel_gap;
-    if (opt_.refine_rounds > 0 && status != PRAMAAN_STATUS_NUMERICAL_FAILURE) refine(res);
     res->primal_weight = omega_;
     res->step_size = eta_;
 }

@@ -147,6 +147,10 @@ void validate_options(const pramaan_pdhg_options& opt) {
         throw InvalidArgument("pdhg options: unknown termination criterion");
     if (opt.algorithm == PRAMAAN_ALGO_REFERENCE && opt.termination != PRAMAAN_TERM_REFERENCE)
         throw InvalidArgument("pdhg options: the reference algorithm uses the reference criterion");
+    if (opt.algorithm == PRAMAAN_ALGO_ADAPTIVE && opt.termination != PRAMAAN_TERM_RELATIVE_KKT)
+        throw InvalidArgument("pdhg options: the adaptive algorithm terminates on the relative KKT error "
+                              "(PRAMAAN_TERM_RELATIVE_KKT)");
+    if (opt.refine != 0 && opt.refine != 1) throw InvalidArgument("pdhg options: refine must be 0 or 1");
 }
 
 PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : opt_(opt) {
@@ -240,6 +244,8 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
         SpmvLauncher<EpiRowKkt, double, float, false>::blocks_per_sm(dev_);
         SpmvLauncher<EpiColKkt, double, float, true>::blocks_per_sm(dev_);
         SpmvLauncher<EpiColKkt, double, float, false>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiStore<double, double>, double, double, true>::blocks_per_sm(dev_);
+        SpmvLauncher<EpiStore<double, double>, double, double, false>::blocks_per_sm(dev_);
         eta_ = 0.99 / estimate_operator_norm();
         // initial primal weight ||C c|| / ||R b|| on the scaled problem
         std::vector<float> hc(static_cast<size_t>(n_)), hr(static_cast<size_t>(m_));
@@ -275,7 +281,7 @@ PdhgEngine::~PdhgEngine() {
 void PdhgEngine::launch_dual() {
     if (m_ <= 0) return;
     if (adaptive_) {
-        EpiDualAdapt epi{sigma_.get(), lr_.get(), ur_.get(), y_.get(), ysum_.get(), scal_.get()};
+        EpiDualAdapt epi{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), ysum_.get(), scal_.get()};
         SpmvLauncher<EpiDualAdapt, float, float, false>::launch(A_.view(false), xbar_.get(), epi,
                                                                 status_.get(), st_, dev_);
         return;
@@ -458,7 +464,7 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
 
     int iter = adaptive_ ? max_it : 0;   // the adaptive loop lives in solve_adaptive
     if (adaptive_) {
-        solve_adaptive(lp, res);
+        solve_adaptive(res);
         restarts = res->restarts;
         numerical_failure = res->status == PRAMAAN_STATUS_NUMERICAL_FAILURE;
     }
@@ -499,7 +505,7 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
     {
         double pv = 0, dv = 0;
         bool nonfinite = false;
-        if (refined_) reference_residuals64(pv, dv, nonfinite);
+        if (master_out_) reference_residuals64(pv, dv, nonfinite);
         else residuals(pv, dv, nonfinite);
         res->primal_residual = pv;
         res->dual_residual = dv;
@@ -507,7 +513,7 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
             res->status = PRAMAAN_STATUS_NUMERICAL_FAILURE;
     }
     std::vector<double> hx(static_cast<size_t>(n_)), hy(static_cast<size_t>(m_));
-    if (refined_) {
+    if (master_out_) {
         // the FP64 master iterate is the answer
         if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(hx.data(), x64_.get(), size_t(n_) * 8, cudaMemcpyDeviceToHost, st_));
         if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(hy.data(), y64_.get(), size_t(m_) * 8, cudaMemcpyDeviceToHost, st_));
@@ -529,7 +535,7 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
     if (res->row_activity && m_ > 0) {
         DevBuf<double> act{size_t(m_)};
         EpiStore<double, double> epi{act.get()};
-        if (refined_) {
+        if (master_out_) {
             if (A_.has_lo)
                 SpmvLauncher<EpiStore<double, double>, double, double, true>::launch(
                     A_.view(true), x64_.get(), epi, status_.get(), st_, dev_);

@@ -60,11 +60,9 @@ public:
         double weighted(double omega) const;          // restart metric
         bool converged(double tol) const { return rel_p <= tol && rel_d <= tol && rel_gap <= tol; }
     };
-    // Relative KKT of the current iterate and of the average (synchronises),
-    // for the problem the FP32 iteration currently solves.
+    // Relative KKT (FP64, original problem) of the current iterate and of the
+    // epoch's average, both as master + correction (synchronises).
     void kkt_pair(Kkt& cur, Kkt& avg);
-    // Relative KKT of the FP64 master iterate on the original problem.
-    void kkt_master(Kkt& k);
     double primal_weight() const { return omega_; }
     double step_size() const { return eta_; }
 
@@ -82,14 +80,14 @@ private:
     void set_weight(double omega);
     void materialize_average();
     void restart_to(bool average);
-    // Runs the adaptive loop on the current problem to `tol` within `max_it`
-    // iterations; returns the PRAMAAN_STATUS_* of the loop.
-    int adaptive_loop(double tol, int max_it, pramaan_solve_result* res, Kkt* last_out);
-    void solve_adaptive(const pramaan_lp& lp, pramaan_solve_result* res);
+    // Folds the correction (d, e) into the FP64 master (x_m, y_m) — or, with
+    // `first`, sets the master to the starting point — and refreshes the FP32
+    // vectors the correction iteration reads; d = e = d̄ = 0 afterwards.
+    void fold(bool first);
+    // x64_ = x_m + d, y64_ = y_m + e; the FP32 vectors back to the original LP.
+    void finish_adaptive();
+    void solve_adaptive(pramaan_solve_result* res);
     double dist2(const float* a, const float* b, const float* scale, int len);
-    // FP64 iterative refinement (pdhg_refine.cu)
-    void refine(pramaan_solve_result* res);
-    void use_original_problem();
     void reference_residuals64(double& pv, double& dv, bool& nonfinite);
 
     int dev_ = 0;
@@ -106,25 +104,21 @@ private:
     double* h_slots_ = nullptr;   // pinned
     int* h_status_ = nullptr;     // pinned
 
-    // adaptive-mode state
+    // adaptive-mode state.  The FP32 iterate buffers hold the correction
+    // (x_ = d, y_ = e, xbar_ = d̄) and the FP32 problem vectors its folded data
+    // (c_ = c + A^T y_m, lr_/ur_ = A x_m - l_r / - u_r, lx_/ux_ = bounds - x_m).
     DevBuf<double> cmin64_, xsum_, ysum_, part_, red_;
     DevBuf<float> rscale_, cscale_, xa_, ya_, xl_, yl_, scal_;
+    DevBuf<double> xm64_, ym64_, actm64_, rcm64_;   // FP64 master, A x_m, c + A^T y_m
+    DevBuf<float> ym32_;
     double* h_red_ = nullptr;     // pinned, kPartSlots
     double eta_ = 1.0, omega_ = 1.0;
     double b_norm_ = 0.0, c_norm2_ = 0.0;
     long long avg_count_ = 0;
-    // The problem the FP32 iteration solves: the original LP, or during FP64
-    // refinement the scaled correction LP (same matrix, new vectors).
-    const double* pc64_ = nullptr;
-    const double* prlo_ = nullptr;
-    const double* prhi_ = nullptr;
-    const double* pvlo_ = nullptr;
-    const double* pvhi_ = nullptr;
-    double pb_norm_ = 0.0, pc_norm_ = 0.0;
-    // FP64 refinement state
-    bool refined_ = false;
-    DevBuf<double> x64_, y64_, act64_, aty64_, cc64_, crlo64_, crhi64_, cvlo64_, cvhi64_;
-    int total_iterations_ = 0;
+    int folds_ = 0;
+    // FP64 answer of an adaptive solve (x_m + d, y_m + e)
+    bool master_out_ = false;
+    DevBuf<double> x64_, y64_;
 
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;

@@ -122,13 +122,12 @@ class PdhgOptions:
     tolerance: float = 1e-6
     max_iterations: int = 100000
     check_frequency: int = 100
-    algorithm: int = 0          # 0: the reference iteration
-    termination: int = 0        # 0: the reference criterion
+    algorithm: int = 0          # 0: the reference iteration, 1: adaptive
+    termination: int | None = None  # default: reference criterion / relative KKT (adaptive)
     device: int = 0
     use_graph: bool = True
     profile_kernels: bool = False
-    refine_rounds: int = 0        # FP64 iterative-refinement rounds (adaptive mode)
-    refine_tolerance: float = 1e-8
+    refine: bool = True         # adaptive mode: FP64 master iterates + FP32 corrections
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -137,12 +136,14 @@ class PdhgOptions:
         o.max_iterations = int(self.max_iterations)
         o.check_frequency = int(self.check_frequency)
         o.algorithm = int(self.algorithm)
-        o.termination = int(self.termination)
+        if self.termination is None:
+            o.termination = TERM_RELATIVE_KKT if int(self.algorithm) == ALGO_ADAPTIVE else TERM_REFERENCE
+        else:
+            o.termination = int(self.termination)
         o.device = int(self.device)
         o.use_graph = int(bool(self.use_graph))
         o.profile_kernels = int(bool(self.profile_kernels))
-        o.refine_rounds = int(self.refine_rounds)
-        o.refine_tolerance = float(self.refine_tolerance)
+        o.refine = int(bool(self.refine))
         return o
 
 

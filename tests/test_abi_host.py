@@ -43,7 +43,7 @@ def test_struct_layouts_match_header():
     # pramaan_lp: 4 int32 + double + 8 pointers; options 64 bytes; result.
     assert C.sizeof(L.CLp) == 4 * 4 + 8 + 8 * 8
     assert C.sizeof(L.COptions) == 8 + 4 * 8 + 8 + 4 * 6
-    assert L.COptions.refine_tolerance.offset == 40
+    assert L.COptions.refine.offset == 36 and L.COptions.reserved_d.offset == 40
     assert L.CResult.restarts.offset == 8 + 3 * 8 + 3 * 8
 
 
@@ -52,7 +52,7 @@ def test_default_options_match_reference(lib):
     lib.pramaan_pdhg_default_options(C.byref(o))
     # include/pramaan/gpu/pdhg_solver.hpp:9-13
     assert o.tolerance == 1e-6 and o.max_iterations == 100000 and o.check_frequency == 100
-    assert o.algorithm == 0 and o.termination == 0
+    assert o.algorithm == 0 and o.termination == 0 and o.refine == 1
     p = PdhgOptions()
     assert (p.tolerance, p.max_iterations, p.check_frequency) == (1e-6, 100000, 100)
 

@@ -145,3 +145,29 @@ def test_oracle_small_random_lp_matches_reference_simplex():
     r = oracle.solve_ref(model, tol=1e-6, max_iterations=200000, check_frequency=100)
     assert r["status"] == 0
     assert abs(r["objective_value"] - cpu["objective_value"]) <= 1e-4 * (1 + abs(cpu["objective_value"]))
+
+
+# ---- the numpy restatement of the adaptive mode (oracle/adaptive.py) ----------
+
+def test_adaptive_restatement_rel_kkt_equals_c_oracle():
+    from oracle import adaptive as ada
+    rng = np.random.default_rng(11)
+    for name in ("wyndor", "multi", "bounded"):
+        model = KNOWN[name][0]
+        x = rng.uniform(-1, 5, model.numVars())
+        y = rng.uniform(-2, 2, model.numRows())
+        mine = ada.rel_kkt(ada.problem(model), x, y)
+        ref = oracle.rel_kkt(model, x, y)
+        for a, b in (("rel_p", "primal"), ("rel_d", "dual"), ("rel_gap", "gap"), ("pobj", "pobj"),
+                     ("dobj", "dobj")):
+            assert mine[a] == pytest.approx(ref[b], rel=1e-12, abs=1e-14), (name, a)
+
+
+@pytest.mark.parametrize("name", ["wyndor", "multi", "equality", "bounded"])
+def test_adaptive_restatement_solves_known_answers(name):
+    from oracle import adaptive as ada
+    model, obj, _ = KNOWN[name]
+    r = ada.solve(model, tol=1e-8, max_iterations=50000)
+    assert r["status"] == "optimal"
+    sgn = -1.0 if int(model.obj_sense) == 1 else 1.0
+    assert sgn * r["kkt"]["pobj"] + model.obj_offset == pytest.approx(obj, rel=1e-7, abs=1e-7)
