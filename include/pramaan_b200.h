@@ -117,7 +117,7 @@ typedef struct pramaan_solve_result {
     double rel_gap;            /*   residual||/(1+||c||), |p-d|/(1+|p|+|d|)     */
     double primal_weight;      /* final omega (adaptive mode)                   */
     double step_size;          /* eta (adaptive mode)                           */
-    double reserved[1];
+    double compactions;        /* batch solves: operand rebuilds during the batch */
 } pramaan_solve_result;
 
 /* Library identification. */
@@ -134,6 +134,23 @@ PRAMAAN_API void pramaan_pdhg_default_options(pramaan_pdhg_options* opt);
  * result.  Returns PRAMAAN_OK when the solve ran (whatever its status). */
 PRAMAAN_API int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
                        pramaan_solve_result* result);
+
+/* Many LPs solved together (no reference counterpart; the batch client of
+ * the reference is PdhgSolver::solve called once per LP, e.g. per
+ * branch-and-bound node relaxation or rolling-horizon window).  The LPs are
+ * packed into one block-diagonal operand, so each half-iteration of all of
+ * them is one kernel launch; each LP keeps its own step size, primal weight,
+ * restarts, FP64 refinement and termination, and is frozen once it meets the
+ * tolerance.  opt->algorithm must be PRAMAAN_ALGO_ADAPTIVE with
+ * PRAMAAN_TERM_RELATIVE_KKT (NULL: the defaults with those two set).
+ * results[k] is LP k's result, with caller-owned x / y / row_activity
+ * buffers as in pramaan_pdhg_solve; solve_ms is the whole batch's time.
+ * LPs without variables or with non-finite costs get the reference's early
+ * answers.  The packed sizes must stay below 2^30 rows, columns and
+ * non-zeros. */
+PRAMAAN_API int pramaan_pdhg_solve_batch(const pramaan_lp* lps, int32_t count,
+                                         const pramaan_pdhg_options* opt,
+                                         pramaan_solve_result* results);
 
 /* ---- test-harness launchers (src/gpu/pdhg.cu:77-241) --------------------- */
 

@@ -47,7 +47,7 @@ class CResult(C.Structure):
         ("x", P), ("row_activity", P), ("y", P),
         ("restarts", i32), ("checks", i32), ("solve_ms", f64),
         ("rel_primal", f64), ("rel_dual", f64), ("rel_gap", f64), ("primal_weight", f64),
-        ("step_size", f64), ("reserved", f64 * 1),
+        ("step_size", f64), ("compactions", f64),
     ]
 
 
@@ -57,6 +57,7 @@ SIGNATURES = [
     ("pramaan_last_error", C.c_char_p, []),
     ("pramaan_pdhg_default_options", None, [C.POINTER(COptions)]),
     ("pramaan_pdhg_solve", C.c_int, [C.POINTER(CLp), C.POINTER(COptions), C.POINTER(CResult)]),
+    ("pramaan_pdhg_solve_batch", C.c_int, [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CResult)]),
     ("pramaan_launch_spmv", C.c_int, [P, P, P, i32, P, P, i32, i32]),
     ("pramaan_launch_spmv_t", C.c_int, [P, P, P, i32, P, P, i32, i32]),
     ("pramaan_launch_pdhg_iteration", C.c_int, [P, P, P, P, P, i32, i32, f32, f32]),

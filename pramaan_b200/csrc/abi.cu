@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.cuh"
 #include "pdhg_engine.cuh"
 
 struct pramaan_pdhg_session {
@@ -158,6 +159,22 @@ void pramaan_pdhg_default_options(pramaan_pdhg_options* opt) {
     if (opt) *opt = defaults();
 }
 
+int pramaan_pdhg_solve_batch(const pramaan_lp* lps, int32_t count, const pramaan_pdhg_options* opt,
+                             pramaan_solve_result* results) {
+    return guarded([&] {
+        if (count < 0) throw InvalidArgument("count must be >= 0");
+        if (count > 0 && (!lps || !results)) throw InvalidArgument("lps and results must not be NULL");
+        pramaan_pdhg_options o = opt ? *opt : defaults();
+        if (!opt) {
+            o.algorithm = PRAMAAN_ALGO_ADAPTIVE;
+            o.termination = PRAMAAN_TERM_RELATIVE_KKT;
+        }
+        DeviceGuard g(o.device);
+        AdaptiveBatch batch(lps, count, o);
+        batch.solve(lps, results);
+    });
+}
+
 int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
                        pramaan_solve_result* res) {
     return guarded([&] {
@@ -168,6 +185,7 @@ int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
         res->iterations = 0;
         res->restarts = 0;
         res->checks = 0;
+        res->compactions = 0.0;
         res->primal_residual = std::numeric_limits<double>::infinity();
         res->dual_residual = std::numeric_limits<double>::infinity();
         res->objective_value = 0.0;

@@ -134,6 +134,11 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st);
 // ---------------------------------------------------------------------------
 int device_sm_count(int dev);
 
+// Launch autotuner: times the store-only product of `A` at 1-4 resident
+// blocks per SM and records the fastest in A.tuned_blocks_per_sm (operands
+// with fewer than 4 tiles per SM keep the default grid).
+void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status);
+
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
 

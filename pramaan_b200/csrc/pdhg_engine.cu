@@ -83,39 +83,6 @@ __global__ void copy_kernel(const float* __restrict__ src, int n, float* __restr
         dst[j] = src[j];
 }
 
-// Launch autotuner: picks the resident blocks per SM for one operand by
-// timing the SpMV (store-only epilogue into scratch, so no iterate changes)
-// at every candidate occupancy, and records the fastest in the operand.
-void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status) {
-    using Epi = EpiStore<float, float>;
-    using Launch = SpmvLauncher<Epi, float, float, false>;
-    if (A.num_tiles < 4 * device_sm_count(dev)) return;   // small operands: default grid
-    const int occ = Launch::blocks_per_sm(dev);
-    DevBuf<float> xs(static_cast<size_t>(A.cols > 0 ? A.cols : 1)), ys(static_cast<size_t>(A.rows));
-    PB_CUDA_CHECK(cudaMemsetAsync(xs.get(), 0, xs.bytes(), st));
-    Epi epi{ys.get()};
-    cudaEvent_t e0, e1;
-    PB_CUDA_CHECK(cudaEventCreate(&e0));
-    PB_CUDA_CHECK(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int best_bps = 0;
-    for (int bps = 1; bps <= occ && bps <= 4; ++bps) {
-        A.tuned_blocks_per_sm = bps;
-        const CsrView v = A.view(false);
-        Launch::launch(v, xs.get(), epi, status, st, dev);   // warm-up
-        PB_CUDA_CHECK(cudaEventRecord(e0, st));
-        for (int r = 0; r < 3; ++r) Launch::launch(v, xs.get(), epi, status, st, dev);
-        PB_CUDA_CHECK(cudaEventRecord(e1, st));
-        PB_CUDA_CHECK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        PB_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best * 0.98f) { best = ms; best_bps = bps; }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    A.tuned_blocks_per_sm = best_bps;
-}
-
 template <typename T>
 void upload(DevBuf<T>& d, const T* h, size_t n, cudaStream_t st) {
     d.alloc(n);

@@ -14,6 +14,9 @@ FP64 (the ModelIR value type).
   any device so the large instance is generated on the GPU in about a second.
 * ``ill_conditioned_lp`` — k non-zeros per column with log-uniform row and
   column scales (the 200,000 x 500,000 precision-ladder workload).
+* ``rolling_horizon_lp`` / ``rolling_horizon_batch`` — production planning
+  over T periods and P products (the batched workload: 512 LPs with
+  T ~ U{24..336}, P ~ U{5..50}).
 """
 from __future__ import annotations
 
@@ -147,3 +150,71 @@ def model_from_tensors(t: dict) -> ModelIR:
         "obj_coeffs", "row_ptr", "col_idx", "values", "row_lower", "row_upper", "var_lower", "var_upper")}
     return ModelIR(h["obj_coeffs"], h["row_ptr"], h["col_idx"], h["values"], h["row_lower"],
                    h["row_upper"], h["var_lower"], h["var_upper"], ObjSense.kMinimize, 0.0)
+
+
+def rolling_horizon_lp(T: int, P: int, seed: int = 0, demand=None, rng=None):
+    """Multi-product production planning over T periods.
+
+    Variables per (product p, period t), in three blocks of P*T (index
+    p*T + t inside a block): produce x >= 0, inventory I >= 0, backlog B >= 0.
+    Rows: inventory balance per (p, t) (row p*T + t, an equality)
+        I[p,t-1] - B[p,t-1] + x[p,t] - I[p,t] + B[p,t] = d[p,t]
+    (no t-1 terms at t = 0) and one shared capacity row per period
+    (row P*T + t):  sum_p x[p,t] <= cap[t].
+    Demand d ~ lognormal(mu=3, sigma=0.5) unless given as a (P, T) array;
+    production, holding and backlog costs ~ U(1, 10) per (p, t);
+    cap[t] = U(0.8, 1.2) * sum_p E[d].  Backlog keeps every instance
+    feasible and positive costs keep it bounded.
+    """
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    PT = P * T
+    if demand is None:
+        demand = rng.lognormal(3.0, 0.5, size=(P, T))
+    demand = np.asarray(demand, np.float64).reshape(P, T)
+    cost = rng.uniform(1.0, 10.0, size=3 * PT)
+    mean_d = np.exp(3.0 + 0.125)
+    cap = rng.uniform(0.8, 1.2, size=T) * P * mean_d
+    p_idx, t_idx = np.divmod(np.arange(PT), T)
+    # balance rows: columns x, I[t-1], I[t], B[t-1], B[t] (ascending)
+    first = t_idx == 0
+    cnt = np.where(first, 3, 5)
+    row_ptr = np.zeros(PT + T + 1, np.int64)
+    row_ptr[1:PT + 1] = np.cumsum(cnt)
+    cols = np.empty(int(row_ptr[PT]), np.int64)
+    vals = np.empty(int(row_ptr[PT]), np.float64)
+    base = row_ptr[:PT]
+    q = np.arange(PT)
+    # first period: x, I, B
+    f = q[first]
+    cols[base[f]], vals[base[f]] = f, 1.0
+    cols[base[f] + 1], vals[base[f] + 1] = PT + f, -1.0
+    cols[base[f] + 2], vals[base[f] + 2] = 2 * PT + f, 1.0
+    g = q[~first]
+    cols[base[g]], vals[base[g]] = g, 1.0
+    cols[base[g] + 1], vals[base[g] + 1] = PT + g - 1, 1.0
+    cols[base[g] + 2], vals[base[g] + 2] = PT + g, -1.0
+    cols[base[g] + 3], vals[base[g] + 3] = 2 * PT + g - 1, -1.0
+    cols[base[g] + 4], vals[base[g] + 4] = 2 * PT + g, 1.0
+    # capacity rows: x[p, t] for p = 0..P-1
+    cap_cols = (np.arange(P)[None, :] * T + np.arange(T)[:, None]).ravel()
+    row_ptr[PT + 1:] = row_ptr[PT] + P * np.arange(1, T + 1)
+    cols = np.concatenate([cols, cap_cols])
+    vals = np.concatenate([vals, np.ones(P * T)])
+    m, n = PT + T, 3 * PT
+    inf = 1e30
+    row_lower = np.concatenate([demand.ravel(), np.full(T, -inf)])
+    row_upper = np.concatenate([demand.ravel(), cap])
+    return ModelIR(cost, row_ptr.astype(np.int32), cols.astype(np.int32), vals, row_lower, row_upper,
+                   np.zeros(n), np.full(n, inf), ObjSense.kMinimize, 0.0)
+
+
+def rolling_horizon_batch(count: int = 512, seed: int = 0, T_range=(24, 336), P_range=(5, 50)):
+    """``count`` rolling-horizon LPs with T ~ U{T_range}, P ~ U{P_range}
+    (inclusive), drawn from one seeded stream."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        T = int(rng.integers(T_range[0], T_range[1] + 1))
+        P = int(rng.integers(P_range[0], P_range[1] + 1))
+        out.append(rolling_horizon_lp(T, P, rng=rng))
+    return out

@@ -166,6 +166,7 @@ class SolveResult:
     rel_gap: float = float("nan")
     primal_weight: float = 1.0
     step_size: float = 1.0
+    compactions: int = 0        # batch solves: operand rebuilds during the batch
 
 
 class PdhgSolver:
@@ -205,6 +206,52 @@ class PdhgSolver:
         res.rel_primal, res.rel_dual, res.rel_gap = cr.rel_primal, cr.rel_dual, cr.rel_gap
         res.primal_weight, res.step_size = cr.primal_weight, cr.step_size
         return res
+
+    def solve_batch(self, models: list[ModelIR]) -> list[SolveResult]:
+        """Solves many LPs in one packed launch sequence (pramaan_pdhg_solve_batch).
+
+        Uses the adaptive algorithm with relative-KKT termination whatever
+        ``options.algorithm`` says; each LP keeps its own step size, weight,
+        restarts and termination.
+        """
+        return solve_batch(models, self.options)
+
+
+def solve_batch(models: list[ModelIR], options: PdhgOptions | None = None) -> list[SolveResult]:
+    """Batched adaptive PDHG over ``models`` (see ``PdhgSolver.solve_batch``)."""
+    opts = options or PdhgOptions()
+    o = opts.c_struct()
+    o.algorithm = ALGO_ADAPTIVE
+    o.termination = TERM_RELATIVE_KKT
+    k = len(models)
+    lps = (L.CLp * max(k, 1))()
+    res = (L.CResult * max(k, 1))()
+    keep = []
+    outs = []
+    for i, model in enumerate(models):
+        lps[i] = model.c_struct()
+        keep.append(model)
+        x, act, y = np.zeros(model.numVars()), np.zeros(model.numRows()), np.zeros(model.numRows())
+        res[i].x, res[i].row_activity, res[i].y = _ptr(x), _ptr(act), _ptr(y)
+        outs.append((x, act, y))
+    L.check(L.lib().pramaan_pdhg_solve_batch(lps, k, C.byref(o), res))
+    out = []
+    for i in range(k):
+        cr = res[i]
+        r = SolveResult()
+        r.status = SolveStatus(cr.status)
+        r.iterations = cr.iterations
+        r.primal_residual, r.dual_residual = cr.primal_residual, cr.dual_residual
+        r.objective_value = cr.objective_value
+        r.x, r.row_activity, r.y = outs[i]
+        if models[i].numVars() == 0:
+            r.x = np.zeros(0)
+        r.restarts, r.checks, r.solve_ms = cr.restarts, cr.checks, cr.solve_ms
+        r.rel_primal, r.rel_dual, r.rel_gap = cr.rel_primal, cr.rel_dual, cr.rel_gap
+        r.primal_weight, r.step_size = cr.primal_weight, cr.step_size
+        r.compactions = int(cr.compactions)
+        out.append(r)
+    return out
 
 
 # ---- test-harness launchers (src/gpu/pdhg.cu:77-241) ------------------------
