@@ -152,6 +152,74 @@ PRAMAAN_API int pramaan_pdhg_solve_batch(const pramaan_lp* lps, int32_t count,
                                          const pramaan_pdhg_options* opt,
                                          pramaan_solve_result* results);
 
+/* A starting point for one LP (no reference counterpart: the reference's
+ * only warm start is the dual simplex basis of BasisState,
+ * include/pramaan/dual_simplex.hpp:63-130).  Also used as a training target
+ * of the warm-start network. */
+typedef struct pramaan_warm_start {
+    const double* x;        /* [n] primal point, or NULL: clamp(0, l, u)          */
+    const double* y;        /* [m] dual point with the solver's sign (the y of a
+                               pramaan_solve_result), or NULL: 0                 */
+    double primal_weight;   /* > 0: initial primal weight; otherwise the default  */
+} pramaan_warm_start;
+
+/* pramaan_pdhg_solve_batch started from given points: LP k starts from
+ * warm[k] (x clamped into its bounds, y as given, omega as given) instead of
+ * the cold start.  warm == NULL is pramaan_pdhg_solve_batch.  The iteration,
+ * restarts and termination are unchanged, so a result is judged exactly as a
+ * cold one. */
+PRAMAAN_API int pramaan_pdhg_solve_batch_warm(const pramaan_lp* lps, int32_t count,
+                                              const pramaan_pdhg_options* opt,
+                                              const pramaan_warm_start* warm,
+                                              pramaan_solve_result* results);
+
+/* ---- learned warm start (no reference counterpart) ------------------------
+ * A bipartite constraint-variable graph network (3 message-passing layers,
+ * hidden width 64, BF16 weights and activations, FP32 accumulation on the
+ * tensor cores) that predicts x, y and the primal weight of each LP of a
+ * batch.  Its parameters are a flat FP32 vector of pramaan_gnn_num_params()
+ * entries (the master copy; the forward pass uses them rounded to BF16).   */
+typedef struct pramaan_gnn pramaan_gnn;
+typedef struct pramaan_gnn_graph pramaan_gnn_graph;
+
+PRAMAAN_API int32_t pramaan_gnn_num_params(void);
+/* A network with seeded He-uniform weights on `device`. */
+PRAMAAN_API int pramaan_gnn_create(int32_t device, uint64_t seed, pramaan_gnn** out);
+PRAMAAN_API int pramaan_gnn_destroy(pramaan_gnn* net);
+PRAMAAN_API int pramaan_gnn_get_params(const pramaan_gnn* net, float* params);
+/* Replaces the parameters and resets the optimiser state. */
+PRAMAAN_API int pramaan_gnn_set_params(pramaan_gnn* net, const float* params);
+/* Packs `count` LPs into a device-resident graph (features, both CSR
+ * orientations).  `targets` (NULL for prediction only) gives each LP's solved
+ * point: x [n], y [m] and a positive primal weight.  LPs without variables
+ * are skipped (they get no prediction). */
+PRAMAAN_API int pramaan_gnn_graph_create(const pramaan_lp* lps, int32_t count,
+                                         const pramaan_warm_start* targets, int32_t device,
+                                         pramaan_gnn_graph** out);
+PRAMAAN_API int pramaan_gnn_graph_destroy(pramaan_gnn_graph* g);
+/* Forward pass; writes LP k's predicted x into x_out[k] ([n], may be NULL),
+ * y into y_out[k] ([m], may be NULL) and its primal weight into omega_out[k]
+ * (x_out, y_out, omega_out may themselves be NULL). */
+PRAMAAN_API int pramaan_gnn_predict(pramaan_gnn* net, const pramaan_gnn_graph* g, double* const* x_out,
+                                    double* const* y_out, double* omega_out);
+/* Forward + backward without an update: *loss and the gradient of the loss
+ * with respect to every parameter (grad [pramaan_gnn_num_params()], may be
+ * NULL).  The graph must have targets. */
+PRAMAAN_API int pramaan_gnn_gradients(pramaan_gnn* net, const pramaan_gnn_graph* g, float* grad,
+                                      double* loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the loss of graph g; *loss
+ * receives the loss before the step. */
+PRAMAAN_API int pramaan_gnn_train_step(pramaan_gnn* net, const pramaan_gnn_graph* g, float learning_rate,
+                                       double* loss);
+/* Number of floats written by pramaan_gnn_forward_trace for graph g. */
+PRAMAAN_API int64_t pramaan_gnn_trace_size(const pramaan_gnn_graph* g);
+/* Forward pass and a copy of every stored activation as FP32, in order:
+ * X_c of layers 1-3 ([m][128] each: h_c input | aggregated h_v), X_v of
+ * layers 1-3 ([n][128]), h_c and h_v after layer 3 ([m][64], [n][64]),
+ * xhat [n], yhat [m], pooled [K][128], rho [K]  (rows in packed order: LP
+ * after LP, LPs without variables left out). */
+PRAMAAN_API int pramaan_gnn_forward_trace(pramaan_gnn* net, const pramaan_gnn_graph* g, float* out);
+
 /* ---- test-harness launchers (src/gpu/pdhg.cu:77-241) --------------------- */
 
 /* y_out[m] = A x for the FP32 CSR (row_ptr[m+1], col_idx[nnz], values[nnz]),

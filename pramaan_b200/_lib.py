@@ -51,6 +51,10 @@ class CResult(C.Structure):
     ]
 
 
+class CWarmStart(C.Structure):
+    _fields_ = [("x", P), ("y", P), ("primal_weight", f64)]
+
+
 # (name, restype, argtypes) for every entry point declared in the header.
 SIGNATURES = [
     ("pramaan_version", C.c_char_p, []),
@@ -58,6 +62,20 @@ SIGNATURES = [
     ("pramaan_pdhg_default_options", None, [C.POINTER(COptions)]),
     ("pramaan_pdhg_solve", C.c_int, [C.POINTER(CLp), C.POINTER(COptions), C.POINTER(CResult)]),
     ("pramaan_pdhg_solve_batch", C.c_int, [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CResult)]),
+    ("pramaan_pdhg_solve_batch_warm", C.c_int,
+     [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CWarmStart), C.POINTER(CResult)]),
+    ("pramaan_gnn_num_params", i32, []),
+    ("pramaan_gnn_create", C.c_int, [i32, C.c_uint64, C.POINTER(P)]),
+    ("pramaan_gnn_destroy", C.c_int, [P]),
+    ("pramaan_gnn_get_params", C.c_int, [P, P]),
+    ("pramaan_gnn_set_params", C.c_int, [P, P]),
+    ("pramaan_gnn_graph_create", C.c_int, [C.POINTER(CLp), i32, C.POINTER(CWarmStart), i32, C.POINTER(P)]),
+    ("pramaan_gnn_graph_destroy", C.c_int, [P]),
+    ("pramaan_gnn_predict", C.c_int, [P, P, P, P, P]),
+    ("pramaan_gnn_gradients", C.c_int, [P, P, P, C.POINTER(f64)]),
+    ("pramaan_gnn_train_step", C.c_int, [P, P, f32, C.POINTER(f64)]),
+    ("pramaan_gnn_trace_size", i64, [P]),
+    ("pramaan_gnn_forward_trace", C.c_int, [P, P, P]),
     ("pramaan_launch_spmv", C.c_int, [P, P, P, i32, P, P, i32, i32]),
     ("pramaan_launch_spmv_t", C.c_int, [P, P, P, i32, P, P, i32, i32]),
     ("pramaan_launch_pdhg_iteration", C.c_int, [P, P, P, P, P, i32, i32, f32, f32]),

@@ -12,10 +12,18 @@
 #include <vector>
 
 #include "batch.cuh"
+#include "gnn.cuh"
 #include "pdhg_engine.cuh"
 
 struct pramaan_pdhg_session {
     std::unique_ptr<pb::PdhgEngine> eng;
+};
+struct pramaan_gnn {
+    int device = 0;
+    std::unique_ptr<pb::GnnModel> model;
+};
+struct pramaan_gnn_graph {
+    std::unique_ptr<pb::GnnGraph> graph;
 };
 
 namespace pb {
@@ -144,6 +152,11 @@ pramaan_pdhg_options defaults() {
     return o;
 }
 
+void same_device(const pramaan_gnn* net, const pramaan_gnn_graph* gr) {
+    if (!net || !gr) throw InvalidArgument("net and graph must not be NULL");
+    if (net->device != gr->graph->device) throw InvalidArgument("net and graph live on different devices");
+}
+
 }  // namespace
 }  // namespace pb
 
@@ -161,6 +174,11 @@ void pramaan_pdhg_default_options(pramaan_pdhg_options* opt) {
 
 int pramaan_pdhg_solve_batch(const pramaan_lp* lps, int32_t count, const pramaan_pdhg_options* opt,
                              pramaan_solve_result* results) {
+    return pramaan_pdhg_solve_batch_warm(lps, count, opt, nullptr, results);
+}
+
+int pramaan_pdhg_solve_batch_warm(const pramaan_lp* lps, int32_t count, const pramaan_pdhg_options* opt,
+                                  const pramaan_warm_start* warm, pramaan_solve_result* results) {
     return guarded([&] {
         if (count < 0) throw InvalidArgument("count must be >= 0");
         if (count > 0 && (!lps || !results)) throw InvalidArgument("lps and results must not be NULL");
@@ -170,7 +188,7 @@ int pramaan_pdhg_solve_batch(const pramaan_lp* lps, int32_t count, const pramaan
             o.termination = PRAMAAN_TERM_RELATIVE_KKT;
         }
         DeviceGuard g(o.device);
-        AdaptiveBatch batch(lps, count, o);
+        AdaptiveBatch batch(lps, count, o, warm);
         batch.solve(lps, results);
     });
 }
@@ -352,6 +370,119 @@ int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual, do
         if (!s) throw InvalidArgument("session is NULL");
         if (bytes_dual) *bytes_dual = s->eng->bytes_dual();
         if (bytes_primal) *bytes_primal = s->eng->bytes_primal();
+    });
+}
+
+// ---- learned warm start --------------------------------------------------
+
+int32_t pramaan_gnn_num_params(void) { return pb::GnnModel::num_params(); }
+
+int pramaan_gnn_create(int32_t device, uint64_t seed, pramaan_gnn** out) {
+    return guarded([&] {
+        if (!out) throw InvalidArgument("out is NULL");
+        *out = nullptr;
+        DeviceGuard g(device);
+        auto n = std::make_unique<pramaan_gnn>();
+        n->device = device;
+        n->model = std::make_unique<GnnModel>(device, seed);
+        *out = n.release();
+    });
+}
+
+int pramaan_gnn_destroy(pramaan_gnn* net) {
+    return guarded([&] {
+        if (!net) return;
+        DeviceGuard g(net->device);
+        delete net;
+    });
+}
+
+int pramaan_gnn_get_params(const pramaan_gnn* net, float* params) {
+    return guarded([&] {
+        if (!net || !params) throw InvalidArgument("net and params must not be NULL");
+        DeviceGuard g(net->device);
+        net->model->get_params(params);
+    });
+}
+
+int pramaan_gnn_set_params(pramaan_gnn* net, const float* params) {
+    return guarded([&] {
+        if (!net || !params) throw InvalidArgument("net and params must not be NULL");
+        DeviceGuard g(net->device);
+        net->model->set_params(params);
+    });
+}
+
+int pramaan_gnn_graph_create(const pramaan_lp* lps, int32_t count, const pramaan_warm_start* targets,
+                             int32_t device, pramaan_gnn_graph** out) {
+    return guarded([&] {
+        if (!out) throw InvalidArgument("out is NULL");
+        *out = nullptr;
+        if (count < 0) throw InvalidArgument("count must be >= 0");
+        if (count > 0 && !lps) throw InvalidArgument("lps is NULL");
+        DeviceGuard g(device);
+        auto h = std::make_unique<pramaan_gnn_graph>();
+        h->graph = std::make_unique<GnnGraph>(lps, count, targets, device);
+        *out = h.release();
+    });
+}
+
+int pramaan_gnn_graph_destroy(pramaan_gnn_graph* gr) {
+    return guarded([&] {
+        if (!gr) return;
+        DeviceGuard g(gr->graph->device);
+        delete gr;
+    });
+}
+
+int pramaan_gnn_predict(pramaan_gnn* net, const pramaan_gnn_graph* gr, double* const* x_out,
+                        double* const* y_out, double* omega_out) {
+    return guarded([&] {
+        same_device(net, gr);
+        DeviceGuard g(net->device);
+        net->model->forward(*gr->graph);
+        net->model->predict(*gr->graph, x_out, y_out, omega_out);
+    });
+}
+
+int pramaan_gnn_gradients(pramaan_gnn* net, const pramaan_gnn_graph* gr, float* grad, double* loss) {
+    return guarded([&] {
+        same_device(net, gr);
+        DeviceGuard g(net->device);
+        net->model->forward(*gr->graph);
+        const double l = net->model->backward(*gr->graph, true);
+        if (loss) *loss = l;
+        if (grad) net->model->copy_grad(grad);
+    });
+}
+
+int pramaan_gnn_train_step(pramaan_gnn* net, const pramaan_gnn_graph* gr, float learning_rate, double* loss) {
+    return guarded([&] {
+        same_device(net, gr);
+        if (!(learning_rate > 0.0f) || !std::isfinite(learning_rate))
+            throw InvalidArgument("learning_rate must be positive and finite");
+        DeviceGuard g(net->device);
+        net->model->forward(*gr->graph);
+        const double l = net->model->backward(*gr->graph, true);
+        net->model->adam_step(learning_rate);
+        if (loss) *loss = l;
+    });
+}
+
+int64_t pramaan_gnn_trace_size(const pramaan_gnn_graph* gr) {
+    if (!gr) return 0;
+    const pb::GnnGraph& g = *gr->graph;
+    return int64_t(pb::kGnnLayers) * (int64_t(g.m) + g.n) * 128 + (int64_t(g.m) + g.n) * 64 + g.n + g.m +
+           int64_t(g.K) * 129;
+}
+
+int pramaan_gnn_forward_trace(pramaan_gnn* net, const pramaan_gnn_graph* gr, float* out) {
+    return guarded([&] {
+        same_device(net, gr);
+        if (!out) throw InvalidArgument("out is NULL");
+        DeviceGuard g(net->device);
+        net->model->forward(*gr->graph);
+        net->model->trace(*gr->graph, out);
     });
 }
 

@@ -85,6 +85,17 @@ __global__ void copy2_kernel(const float* __restrict__ src, int n, float* __rest
 }
 
 // Starting master: x_m = clamp(0, l_x, u_x) (the reference's x0), y_m = 0.
+// xm = clamp(xw, l, u): the FP64 master iterate of a warm start.
+__global__ void init_master_warm_kernel(const double* __restrict__ xw, const double* __restrict__ vlo,
+                                        const double* __restrict__ vhi, int n, double* __restrict__ xm) {
+    PB_GRID_STRIDE(j, n) {
+        double v = xw[j];
+        if (vhi[j] < kInf && v > vhi[j]) v = vhi[j];
+        if (vlo[j] > -kInf && v < vlo[j]) v = vlo[j];
+        xm[j] = v;
+    }
+}
+
 __global__ void init_master_kernel(const double* __restrict__ vlo, const double* __restrict__ vhi, int n,
                                    double* __restrict__ xm) {
     PB_GRID_STRIDE(j, n) {

@@ -325,7 +325,9 @@ double weighted(double pr2, double dr2, double gap, double omega) {
 
 }  // namespace
 
-AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdhg_options& opt) : opt_(opt) {
+AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdhg_options& opt,
+                             const pramaan_warm_start* warm)
+    : opt_(opt) {
     validate_options(opt);
     if (opt.algorithm != PRAMAAN_ALGO_ADAPTIVE)
         throw InvalidArgument("batched solves use the adaptive algorithm (PRAMAAN_ALGO_ADAPTIVE)");
@@ -402,6 +404,26 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     }
     rp[m_] = int(e0);
     rseg[K_] = m_; cseg[K_] = n_;
+    std::vector<double> xw, yw;
+    if (warm) {
+        xw.assign(N, 0.0);
+        yw.assign(M, 0.0);
+        for (int q = 0; q < K_; ++q) {
+            const Lp& s = lp_[q];
+            const pramaan_warm_start& w = warm[s.index];
+            const int nk = s.c1 - s.c0, mk = s.r1 - s.r0;
+            for (int j = 0; j < nk; ++j) {
+                const double v = w.x ? w.x[j] : 0.0;
+                if (!std::isfinite(v)) throw InvalidArgument("warm start: x must be finite");
+                xw[size_t(s.c0 + j)] = v;
+            }
+            for (int i = 0; i < mk; ++i) {
+                const double v = w.y ? w.y[i] : 0.0;
+                if (!std::isfinite(v)) throw InvalidArgument("warm start: y must be finite");
+                yw[size_t(s.r0 + i)] = v;
+            }
+        }
+    }
 
     PB_CUDA_CHECK(cudaMallocHost(&h_action_, sizeof(int) * K_));
     PB_CUDA_CHECK(cudaMallocHost(&h_inv_, sizeof(double) * K_));
@@ -430,6 +452,7 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     };
     up(cmin64_, cmin); up(rlo64_, rl); up(rhi64_, ru); up(vlo64_, vl); up(vhi64_, vu);
     up(lp_row_, lp_row); up(lp_col_, lp_col);
+    if (warm) { up(xw_, xw); up(yw_, yw); }
     build_segments(rseg_, rseg);
     build_segments(cseg_, cseg);
     c_.alloc(n_); lx_.alloc(n_); ux_.alloc(n_); tau0_.alloc(n_); tau_.alloc(n_); x_.alloc(n_); xbar_.alloc(n_);
@@ -483,6 +506,10 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
         cs = std::sqrt(cs);
         bs = std::sqrt(bs);
         s.omega = cs > 1e-10 && bs > 1e-10 ? cs / bs : 1.0;
+        if (warm) {
+            const double w = warm[s.index].primal_weight;
+            if (w > 0.0 && std::isfinite(w)) s.omega = w;
+        }
     }
     apply_steps();
     PB_CUDA_CHECK(cudaStreamSynchronize(st_));
@@ -736,8 +763,16 @@ void AdaptiveBatch::push_actions() {
 
 void AdaptiveBatch::fold(bool first) {
     if (first) {
-        init_master_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(vlo64_.get(), vhi64_.get(), n_, xm64_.get());
-        if (m_) PB_CUDA_CHECK(cudaMemsetAsync(ym64_.get(), 0, ym64_.bytes(), st_));
+        if (xw_.size()) {
+            init_master_warm_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(xw_.get(), vlo64_.get(), vhi64_.get(), n_,
+                                                                       xm64_.get());
+            if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(ym64_.get(), yw_.get(), ym64_.bytes(), cudaMemcpyDeviceToDevice, st_));
+            xw_.reset();
+            yw_.reset();
+        } else {
+            init_master_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(vlo64_.get(), vhi64_.get(), n_, xm64_.get());
+            if (m_) PB_CUDA_CHECK(cudaMemsetAsync(ym64_.get(), 0, ym64_.bytes(), st_));
+        }
         PB_CUDA_CHECK(cudaMemsetAsync(x_.get(), 0, x_.bytes(), st_));
         PB_CUDA_CHECK(cudaMemsetAsync(xbar_.get(), 0, xbar_.bytes(), st_));
         if (m_) PB_CUDA_CHECK(cudaMemsetAsync(y_.get(), 0, y_.bytes(), st_));

@@ -36,7 +36,10 @@ namespace pb {
 
 class AdaptiveBatch {
 public:
-    AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdhg_options& opt);
+    // `warm` (may be NULL) gives LP k's starting point warm[k]; NULL members
+    // keep the cold start for that part.
+    AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdhg_options& opt,
+                  const pramaan_warm_start* warm = nullptr);
     ~AdaptiveBatch();
     AdaptiveBatch(const AdaptiveBatch&) = delete;
     AdaptiveBatch& operator=(const AdaptiveBatch&) = delete;
@@ -125,6 +128,7 @@ private:
     DevBuf<double> xsum_, ysum_, xm64_, ym64_, actm64_, rcm64_;
     DevBuf<double> rcon_, ccon_, chunk_out_, lp_out_;
     DevBuf<int> action_;
+    DevBuf<double> xw_, yw_;           // warm start (original layout), empty when cold
     DevBuf<double> inv_;
     DevBuf<float> dscale_, pscale_, lp_f_;
     // pinned host mirrors of the per-LP arrays

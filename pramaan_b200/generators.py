@@ -152,7 +152,7 @@ def model_from_tensors(t: dict) -> ModelIR:
                    h["row_upper"], h["var_lower"], h["var_upper"], ObjSense.kMinimize, 0.0)
 
 
-def rolling_horizon_lp(T: int, P: int, seed: int = 0, demand=None, rng=None):
+def rolling_horizon_lp(T: int, P: int, seed: int = 0, demand=None, rng=None, cost=None, cap=None):
     """Multi-product production planning over T periods.
 
     Variables per (product p, period t), in three blocks of P*T (index
@@ -162,8 +162,9 @@ def rolling_horizon_lp(T: int, P: int, seed: int = 0, demand=None, rng=None):
     (no t-1 terms at t = 0) and one shared capacity row per period
     (row P*T + t):  sum_p x[p,t] <= cap[t].
     Demand d ~ lognormal(mu=3, sigma=0.5) unless given as a (P, T) array;
-    production, holding and backlog costs ~ U(1, 10) per (p, t);
-    cap[t] = U(0.8, 1.2) * sum_p E[d].  Backlog keeps every instance
+    production, holding and backlog costs ~ U(1, 10) per (p, t) unless given
+    (3 blocks of P*T, index p*T + t); cap[t] = U(0.8, 1.2) * sum_p E[d]
+    unless given.  Backlog keeps every instance
     feasible and positive costs keep it bounded.
     """
     rng = rng if rng is not None else np.random.default_rng(seed)
@@ -171,9 +172,13 @@ def rolling_horizon_lp(T: int, P: int, seed: int = 0, demand=None, rng=None):
     if demand is None:
         demand = rng.lognormal(3.0, 0.5, size=(P, T))
     demand = np.asarray(demand, np.float64).reshape(P, T)
-    cost = rng.uniform(1.0, 10.0, size=3 * PT)
+    if cost is None:
+        cost = rng.uniform(1.0, 10.0, size=3 * PT)
+    cost = np.asarray(cost, np.float64).reshape(3 * PT)
     mean_d = np.exp(3.0 + 0.125)
-    cap = rng.uniform(0.8, 1.2, size=T) * P * mean_d
+    if cap is None:
+        cap = rng.uniform(0.8, 1.2, size=T) * P * mean_d
+    cap = np.asarray(cap, np.float64).reshape(T)
     p_idx, t_idx = np.divmod(np.arange(PT), T)
     # balance rows: columns x, I[t-1], I[t], B[t-1], B[t] (ascending)
     first = t_idx == 0
@@ -217,4 +222,37 @@ def rolling_horizon_batch(count: int = 512, seed: int = 0, T_range=(24, 336), P_
         T = int(rng.integers(T_range[0], T_range[1] + 1))
         P = int(rng.integers(P_range[0], P_range[1] + 1))
         out.append(rolling_horizon_lp(T, P, rng=rng))
+    return out
+
+
+def rolling_horizon_stream(count: int, seed: int = 0, T: int | None = None, P: int | None = None,
+                           T_range=(24, 336), P_range=(5, 50), phi: float = 0.9, sigma: float = 0.1):
+    """``count`` consecutive windows of one production-planning stream.
+
+    Window k is ``rolling_horizon_lp`` over periods k .. k+T-1 of one long
+    horizon (the window shifts by one period from LP to LP).  T and P are
+    drawn from the batch ranges unless given.  Demand of product p in period
+    t is mu_p exp(u_{p,t}) with mu_p ~ lognormal(3, 0.5) and u an AR(1)
+    process, u_t = phi u_{t-1} + sigma e_t (stationary start); production,
+    holding and backlog costs ~ U(1, 10) and the capacity
+    U(0.8, 1.2) * sum_p E[d] are drawn per period of the long horizon, so
+    consecutive windows share all but one period of their data."""
+    rng = np.random.default_rng(seed)
+    T = int(rng.integers(T_range[0], T_range[1] + 1)) if T is None else int(T)
+    P = int(rng.integers(P_range[0], P_range[1] + 1)) if P is None else int(P)
+    L = T + count - 1
+    mu = rng.lognormal(3.0, 0.5, size=P)
+    u = np.empty((P, L))
+    u[:, 0] = rng.normal(0.0, sigma / np.sqrt(1.0 - phi * phi), size=P)
+    eps = rng.normal(0.0, sigma, size=(P, L))
+    for t in range(1, L):
+        u[:, t] = phi * u[:, t - 1] + eps[:, t]
+    demand = mu[:, None] * np.exp(u)
+    cost = rng.uniform(1.0, 10.0, size=(3, P, L))
+    cap = rng.uniform(0.8, 1.2, size=L) * P * np.exp(3.0 + 0.125)
+    out = []
+    for k in range(count):
+        sl = slice(k, k + T)
+        out.append(rolling_horizon_lp(T, P, demand=demand[:, sl], cost=cost[:, :, sl].reshape(-1),
+                                      cap=cap[sl]))
     return out

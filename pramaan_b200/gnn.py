@@ -1,0 +1,218 @@
+"""Learned warm start for the batched PDHG: the graph network and its use.
+
+``WarmStartNet`` wraps the network of libpramaan_b200 (pramaan_gnn_*): a
+bipartite constraint-variable graph network with BF16 weights whose forward
+and backward passes are hand-written sm_100a kernels (tensor-core dense
+layers).  ``warm_solve_batch`` is the pipeline: predict (x, y, omega) for every
+LP, solve the batch from those points, and re-solve cold any LP whose warm
+solve did not reach the tolerance — plain cold-start PDHG is the fallback, and
+every answer is judged by the same relative-KKT certificate as a cold solve.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .pdhg import ModelIR, PdhgOptions, SolveResult, SolveStatus, _f64, _ptr, solve_batch
+
+
+@dataclass
+class WarmStart:
+    """A starting point for one LP (pramaan_warm_start)."""
+    x: np.ndarray | None = None
+    y: np.ndarray | None = None
+    primal_weight: float = 0.0
+
+    @staticmethod
+    def from_result(r: SolveResult) -> "WarmStart":
+        return WarmStart(np.asarray(r.x, np.float64), np.asarray(r.y, np.float64), float(r.primal_weight))
+
+
+def _warm_array(models, points):
+    k = len(models)
+    arr = (L.CWarmStart * max(k, 1))()
+    keep = []
+    for i, w in enumerate(points):
+        if w is None:
+            raise ValueError("every LP needs a target point")
+        x = _f64(w.x)
+        y = _f64(w.y) if w.y is not None else np.zeros(0)
+        if len(x) != models[i].numVars() or (models[i].numRows() and len(y) != models[i].numRows()):
+            raise ValueError("target point has the wrong length")
+        keep.extend([x, y])
+        arr[i].x, arr[i].y, arr[i].primal_weight = _ptr(x), _ptr(y), float(w.primal_weight)
+    return arr, keep
+
+
+class GnnGraph:
+    """A batch of LPs packed for the network on one device (pramaan_gnn_graph)."""
+
+    def __init__(self, models: list[ModelIR], targets: list[WarmStart] | None = None, device: int = 0):
+        self.models = list(models)
+        self.device = device
+        k = len(self.models)
+        lps = (L.CLp * max(k, 1))()
+        for i, md in enumerate(self.models):
+            lps[i] = md.c_struct()
+        tptr, keep = (None, [])
+        if targets is not None:
+            if len(targets) != k:
+                raise ValueError("one target per model")
+            tptr, keep = _warm_array(self.models, targets)
+        h = C.c_void_p()
+        L.check(L.lib().pramaan_gnn_graph_create(lps, k, tptr, device, C.byref(h)))
+        self.handle = h
+        del keep
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib().pramaan_gnn_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def trace_size(self) -> int:
+        return int(L.lib().pramaan_gnn_trace_size(self.handle))
+
+
+class WarmStartNet:
+    """The warm-start network on one device (pramaan_gnn)."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        L.check(L.lib().pramaan_gnn_create(device, C.c_uint64(seed), C.byref(h)))
+        self.handle = h
+
+    @staticmethod
+    def num_params() -> int:
+        return int(L.lib().pramaan_gnn_num_params())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib().pramaan_gnn_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- parameters ----
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), np.float32)
+        L.check(L.lib().pramaan_gnn_get_params(self.handle, _ptr(p)))
+        return p
+
+    @params.setter
+    def params(self, value):
+        p = np.ascontiguousarray(np.asarray(value, np.float32))
+        if p.shape != (self.num_params(),):
+            raise ValueError(f"expected {self.num_params()} parameters")
+        L.check(L.lib().pramaan_gnn_set_params(self.handle, _ptr(p)))
+
+    def save(self, path) -> None:
+        np.savez(path, params=self.params)
+
+    def load(self, path) -> None:
+        self.params = np.load(path)["params"]
+
+    # ---- graphs ----
+    def graph(self, models, targets=None) -> GnnGraph:
+        return GnnGraph(models, targets, self.device)
+
+    # ---- inference / training ----
+    def predict(self, models_or_graph) -> list[WarmStart | None]:
+        """Predicted starting point of every LP (None for LPs without variables)."""
+        g = models_or_graph if isinstance(models_or_graph, GnnGraph) else self.graph(models_or_graph)
+        models = g.models
+        k = len(models)
+        xs = [np.zeros(md.numVars()) for md in models]
+        ys = [np.zeros(md.numRows()) for md in models]
+        xp = (C.c_void_p * max(k, 1))(*[_ptr(x) for x in xs])
+        yp = (C.c_void_p * max(k, 1))(*[_ptr(y) for y in ys])
+        om = np.zeros(max(k, 1))
+        L.check(L.lib().pramaan_gnn_predict(self.handle, g.handle, xp, yp, _ptr(om)))
+        return [WarmStart(xs[i], ys[i], float(om[i])) if models[i].numVars() else None for i in range(k)]
+
+    def gradients(self, g: GnnGraph) -> tuple[float, np.ndarray]:
+        grad = np.zeros(self.num_params(), np.float32)
+        loss = C.c_double()
+        L.check(L.lib().pramaan_gnn_gradients(self.handle, g.handle, _ptr(grad), C.byref(loss)))
+        return loss.value, grad
+
+    def train_step(self, g: GnnGraph, lr: float = 1e-3) -> float:
+        loss = C.c_double()
+        L.check(L.lib().pramaan_gnn_train_step(self.handle, g.handle, C.c_float(lr), C.byref(loss)))
+        return loss.value
+
+    def trace(self, g: GnnGraph) -> np.ndarray:
+        out = np.zeros(max(g.trace_size, 1), np.float32)
+        L.check(L.lib().pramaan_gnn_forward_trace(self.handle, g.handle, _ptr(out)))
+        return out[:g.trace_size]
+
+    def fit(self, graphs: list[GnnGraph], epochs: int = 10, lr: float = 1e-3, lr_decay: float = 1.0,
+            seed: int = 0) -> list[float]:
+        """Adam over the given mini-batch graphs; returns the mean loss of each epoch."""
+        rng = np.random.default_rng(seed)
+        hist = []
+        for e in range(epochs):
+            order = rng.permutation(len(graphs))
+            losses = [self.train_step(graphs[i], lr * lr_decay ** e) for i in order]
+            hist.append(float(np.mean(losses)))
+        return hist
+
+
+def training_targets(results: list[SolveResult]) -> list[WarmStart]:
+    return [WarmStart.from_result(r) for r in results]
+
+
+@dataclass
+class WarmSolveInfo:
+    warm_iterations: list[int]
+    fallbacks: int
+    predict_s: float
+    solve_s: float
+    fallback_s: float
+
+
+def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOptions,
+                     fallback_iterations: int | None = None) -> tuple[list[SolveResult], WarmSolveInfo]:
+    """Learned warm start, then cold-start fallback.
+
+    The network predicts (x, y, omega) for every LP, the batch is solved from
+    those points, and every LP whose warm solve is not optimal (it hit
+    ``options.max_iterations``) is solved again from the cold start with
+    ``fallback_iterations`` (default: the same limit).  The returned result of
+    each LP is whichever solve reached the tolerance; both are judged by the
+    same relative-KKT criterion."""
+    import time
+
+    t0 = time.perf_counter()
+    warm = net.predict(models)
+    t1 = time.perf_counter()
+    res = solve_batch(models, options, warm=warm)
+    t2 = time.perf_counter()
+    warm_its = [r.iterations for r in res]
+    bad = [i for i, r in enumerate(res) if r.status != SolveStatus.kOptimal and models[i].numVars() > 0]
+    if bad:
+        o = dataclasses.replace(options)
+        if fallback_iterations:
+            o.max_iterations = fallback_iterations
+        cold = solve_batch([models[i] for i in bad], o)
+        for i, r in zip(bad, cold):
+            if r.status == SolveStatus.kOptimal or res[i].status != SolveStatus.kOptimal:
+                res[i] = r
+    t3 = time.perf_counter()
+    return res, WarmSolveInfo(warm_its, len(bad), t1 - t0, t2 - t1, t3 - t2)

@@ -217,8 +217,14 @@ class PdhgSolver:
         return solve_batch(models, self.options)
 
 
-def solve_batch(models: list[ModelIR], options: PdhgOptions | None = None) -> list[SolveResult]:
-    """Batched adaptive PDHG over ``models`` (see ``PdhgSolver.solve_batch``)."""
+def solve_batch(models: list[ModelIR], options: PdhgOptions | None = None,
+                warm: list | None = None) -> list[SolveResult]:
+    """Batched adaptive PDHG over ``models`` (see ``PdhgSolver.solve_batch``).
+
+    ``warm`` (optional) gives each LP a starting point: an object with
+    attributes ``x``, ``y`` (arrays or None) and ``primal_weight`` (a float,
+    <= 0 for the default), or None for a cold start
+    (pramaan_pdhg_solve_batch_warm)."""
     opts = options or PdhgOptions()
     o = opts.c_struct()
     o.algorithm = ALGO_ADAPTIVE
@@ -234,7 +240,26 @@ def solve_batch(models: list[ModelIR], options: PdhgOptions | None = None) -> li
         x, act, y = np.zeros(model.numVars()), np.zeros(model.numRows()), np.zeros(model.numRows())
         res[i].x, res[i].row_activity, res[i].y = _ptr(x), _ptr(act), _ptr(y)
         outs.append((x, act, y))
-    L.check(L.lib().pramaan_pdhg_solve_batch(lps, k, C.byref(o), res))
+    wptr = None
+    if warm is not None:
+        if len(warm) != k:
+            raise ValueError("solve_batch: warm must have one entry per model")
+        ws = (L.CWarmStart * max(k, 1))()
+        for i, w in enumerate(warm):
+            if w is None:
+                ws[i].x, ws[i].y, ws[i].primal_weight = None, None, 0.0
+                continue
+            wx = None if getattr(w, "x", None) is None else _f64(w.x)
+            wy = None if getattr(w, "y", None) is None else _f64(w.y)
+            if wx is not None and len(wx) != models[i].numVars():
+                raise ValueError("solve_batch: warm x has the wrong length")
+            if wy is not None and len(wy) != models[i].numRows():
+                raise ValueError("solve_batch: warm y has the wrong length")
+            keep.extend([wx, wy])
+            ws[i].x, ws[i].y = _ptr(wx), _ptr(wy)
+            ws[i].primal_weight = float(getattr(w, "primal_weight", 0.0) or 0.0)
+        wptr = ws
+    L.check(L.lib().pramaan_pdhg_solve_batch_warm(lps, k, C.byref(o), wptr, res))
     out = []
     for i in range(k):
         cr = res[i]
