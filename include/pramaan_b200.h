@@ -173,11 +173,39 @@ PRAMAAN_API int pramaan_pdhg_solve_batch_warm(const pramaan_lp* lps, int32_t cou
                                               const pramaan_warm_start* warm,
                                               pramaan_solve_result* results);
 
+/* ---- certificates -----------------------------------------------------------
+ * FP64 certificate of a point (x, y) of an LP, computed on the GPU.  The first
+ * three fields are the reference certificate's (pramaan::generate_certificate,
+ * src/certificate/certificate.cpp:23-107: objective, maximum row violation,
+ * maximum variable-bound violation; integrality is 0 for LPs); the rest add
+ * the dual side the reference leaves empty (std::nullopt there): the relative
+ * KKT error of (x, y) in FP64 with the problem in minimisation form and y the
+ * solver's dual (the negated multiplier). */
+typedef struct pramaan_certificate {
+    double objective_value;    /* c^T x + obj_offset in the model's sense       */
+    double primal_residual;    /* max over rows of max(l_r - Ax, Ax - u_r, 0)    */
+    double bound_violation;    /* max over columns of max(l_x - x, x - u_x, 0)   */
+    double rel_primal;         /* ||(dist(Ax,[l_r,u_r]), dist(x,[l_x,u_x]))||_2
+                                  / (1 + ||finite row bounds||_2)               */
+    double rel_dual;           /* ||rc - proj(rc)||_2 / (1 + ||c||_2), rc = c + A^T y */
+    double rel_gap;            /* |p - d| / (1 + |p| + |d|)                      */
+    double primal_objective;   /* p = c^T x (minimisation form)                  */
+    double dual_objective;     /* d (minimisation form)                          */
+    double kkt;                /* max(rel_primal, rel_dual, rel_gap)             */
+} pramaan_certificate;
+
+/* Certificates of num_points points of each of `count` LPs: points[p * count
+ * + k] is point p of LP k (x NULL: the solver's cold start clamp(0, l, u);
+ * y NULL: 0) and its certificate goes to out[p * count + k].  The LPs are
+ * packed once for all points. */
+PRAMAAN_API int pramaan_certify_batch(const pramaan_lp* lps, int32_t count, const pramaan_warm_start* points,
+                                      int32_t num_points, int32_t device, pramaan_certificate* out);
+
 /* ---- learned warm start (no reference counterpart) ------------------------
  * A bipartite constraint-variable graph network (3 message-passing layers,
  * hidden width 64, BF16 weights and activations, FP32 accumulation on the
  * tensor cores) that predicts x, y and the primal weight of each LP of a
- * batch.  Its parameters are a flat FP32 vector of pramaan_gnn_num_params()
+ * batch, optionally refining a caller-given hint.  Its parameters are a flat FP32 vector of pramaan_gnn_num_params()
  * entries (the master copy; the forward pass uses them rounded to BF16).   */
 typedef struct pramaan_gnn pramaan_gnn;
 typedef struct pramaan_gnn_graph pramaan_gnn_graph;
@@ -190,10 +218,15 @@ PRAMAAN_API int pramaan_gnn_get_params(const pramaan_gnn* net, float* params);
 /* Replaces the parameters and resets the optimiser state. */
 PRAMAAN_API int pramaan_gnn_set_params(pramaan_gnn* net, const float* params);
 /* Packs `count` LPs into a device-resident graph (features, both CSR
- * orientations).  `targets` (NULL for prediction only) gives each LP's solved
- * point: x [n], y [m] and a positive primal weight.  LPs without variables
- * are skipped (they get no prediction). */
+ * orientations).  `hints` (NULL: none) gives each LP an optional prior guess
+ * of its solution (x and / or y, NULL members allowed; the primal weight is
+ * ignored) — for a rolling-horizon stream, the previous window's solution
+ * shifted by one period; the network reads it as node features and predicts
+ * a correction to it.  `targets` (NULL for prediction only) gives each LP's
+ * solved point: x [n], y [m] and a positive primal weight.  LPs without
+ * variables are skipped (they get no prediction). */
 PRAMAAN_API int pramaan_gnn_graph_create(const pramaan_lp* lps, int32_t count,
+                                         const pramaan_warm_start* hints,
                                          const pramaan_warm_start* targets, int32_t device,
                                          pramaan_gnn_graph** out);
 PRAMAAN_API int pramaan_gnn_graph_destroy(pramaan_gnn_graph* g);

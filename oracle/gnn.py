@@ -21,14 +21,15 @@ from __future__ import annotations
 import numpy as np
 
 H = 64
-FEAT = 8
+FEAT = 9
 LAYERS = 3
+LOSS_FLOOR = 1e-2
 
 # flat parameter layout (gnn.cuh GnnParams)
 VIN_W = 0
-VIN_B = VIN_W + 64 * 8
+VIN_B = VIN_W + 64 * FEAT
 CIN_W = VIN_B + 64
-CIN_B = CIN_W + 64 * 8
+CIN_B = CIN_W + 64 * FEAT
 LAYER0 = CIN_B + 64
 DENSE_W = 64 * 128
 LAYER_STRIDE = 2 * (DENSE_W + 64)
@@ -57,7 +58,7 @@ def bf16(a) -> np.ndarray:
 class Graph:
     """Packed batch of LPs (LPs without variables are skipped), as GnnGraph."""
 
-    def __init__(self, models, targets=None):
+    def __init__(self, models, targets=None, hints=None):
         self.index = [k for k, md in enumerate(models) if md.numVars() > 0]
         ms = [models[k] for k in self.index]
         self.K = len(ms)
@@ -101,6 +102,23 @@ class Graph:
         sa_e = self.s_a[self.lp_row[self.rows]] if len(self.rows) else np.zeros(0)
         self.coef_r = self.vals / (sa_e * np.maximum(1, self.deg_r[self.rows]))
         self.coef_c = self.vals / (sa_e * np.maximum(1, self.deg_c[self.cols]))
+        self.base_x, self.base_y = np.zeros(self.n), np.zeros(self.m)
+        self.hint_x, self.hint_y = np.zeros(self.n, bool), np.zeros(self.m, bool)
+        if hints is not None:
+            for q, k in enumerate(self.index):
+                h = hints[k]
+                if h is None:
+                    continue
+                sa, sb, sc = self.s_a[q], self.s_b[q], self.s_c[q]
+                if h.x is not None:
+                    self.base_x[self.c0[q]:self.c0[q + 1]] = np.asarray(h.x) * sa / sb
+                    self.hint_x[self.c0[q]:self.c0[q + 1]] = True
+                if h.y is not None and self.r0[q + 1] > self.r0[q]:
+                    self.base_y[self.r0[q]:self.r0[q + 1]] = np.asarray(h.y) * sa / sc
+                    self.hint_y[self.r0[q]:self.r0[q + 1]] = True
+        # the device adds the hint terms in FP32
+        self.base_x = self.base_x.astype(np.float32).astype(np.float64)
+        self.base_y = self.base_y.astype(np.float32).astype(np.float64)
         self.fv, self.fc = self._features()
         self.has_targets = targets is not None
         if targets is not None:
@@ -113,31 +131,41 @@ class Graph:
                     ty[self.r0[q]:self.r0[q + 1]] = np.asarray(t.y) * sa / sc
                 tw[q] = np.log(t.primal_weight / self.omega_ref[q])
             self.tx, self.ty, self.tw = tx, ty, tw
+            # per-LP loss weights (float32 on the device)
+            nk, mk = np.diff(self.c0), np.diff(self.r0)
+            tx32, ty32 = tx.astype(np.float32).astype(np.float64), ty.astype(np.float32).astype(np.float64)
+            sx = np.bincount(self.lp_col, weights=tx32 ** 2, minlength=self.K)
+            sy = np.bincount(self.lp_row, weights=ty32 ** 2, minlength=self.K)
+            self.lw_x = (1.0 / (nk * (sx / nk + LOSS_FLOOR))).astype(np.float32).astype(np.float64)
+            self.lw_y = np.where(mk > 0, 1.0 / (np.maximum(mk, 1) * (sy / np.maximum(mk, 1) + LOSS_FLOOR)), 0.0)
+            self.lw_y = self.lw_y.astype(np.float32).astype(np.float64)
 
     def _features(self):
         clip = lambda v: np.clip(v, -10.0, 10.0)  # noqa: E731
         sa_c, sb_c, sc_c = self.s_a[self.lp_col], self.s_b[self.lp_col], self.s_c[self.lp_col]
         absum_c = np.bincount(self.cols, weights=np.abs(self.vals), minlength=self.n)
         fl, fu = self.vlo > -1e29, self.vhi < 1e29
-        fv = np.zeros((self.n, 8))
+        fv = np.zeros((self.n, FEAT))
         fv[:, 0] = self.cost / sc_c
         fv[:, 1], fv[:, 2] = fl, fu
         fv[:, 3] = np.where(fl, clip(np.where(fl, self.vlo, 0) * sa_c / sb_c), 0)
         fv[:, 4] = np.where(fu, clip(np.where(fu, self.vhi, 0) * sa_c / sb_c), 0)
         fv[:, 5] = np.log1p(self.deg_c) / 4.0
         fv[:, 6] = np.where(self.deg_c > 0, absum_c / (sa_c * np.maximum(self.deg_c, 1)), 0)
-        fv[:, 7] = 1.0
+        fv[:, 7] = self.hint_x
+        fv[:, 8] = clip(self.base_x)
         sa_r, sb_r = self.s_a[self.lp_row], self.s_b[self.lp_row]
         absum_r = np.bincount(self.rows, weights=np.abs(self.vals), minlength=self.m)
         fl, fu = self.rlo > -1e29, self.rhi < 1e29
-        fc = np.zeros((self.m, 8))
+        fc = np.zeros((self.m, FEAT))
         fc[:, 0] = fl & fu & (self.rlo == self.rhi)
         fc[:, 1], fc[:, 2] = fl, fu
         fc[:, 3] = np.where(fl, clip(np.where(fl, self.rlo, 0) / sb_r), 0)
         fc[:, 4] = np.where(fu, clip(np.where(fu, self.rhi, 0) / sb_r), 0)
         fc[:, 5] = np.log1p(self.deg_r) / 4.0
         fc[:, 6] = np.where(self.deg_r > 0, absum_r / (sa_r * np.maximum(self.deg_r, 1)), 0)
-        fc[:, 7] = 1.0
+        fc[:, 7] = self.hint_y
+        fc[:, 8] = clip(self.base_y)
         return fv.astype(np.float32), fc.astype(np.float32)
 
 
@@ -166,8 +194,8 @@ def forward(params, g: Graph, exact: bool = False) -> dict:
     ar = _Arith(exact)
     p = ar.r(np.asarray(params, np.float32) if not exact else np.asarray(params, np.float64))
     fv, fc = ar.a(g.fv), ar.a(g.fc)
-    wv, bv = p[VIN_W:VIN_B].reshape(64, 8), p[VIN_B:VIN_B + 64]
-    wc, bc = p[CIN_W:CIN_B].reshape(64, 8), p[CIN_B:CIN_B + 64]
+    wv, bv = p[VIN_W:VIN_B].reshape(64, FEAT), p[VIN_B:VIN_B + 64]
+    wc, bc = p[CIN_W:CIN_B].reshape(64, FEAT), p[CIN_B:CIN_B + 64]
     hv = ar.r(np.maximum(fv @ wv.T + bv, 0))
     hc = ar.r(np.maximum(fc @ wc.T + bc, 0))
     act = {"hv0": hv, "hc0": hc, "xc": [], "xv": []}
@@ -183,8 +211,8 @@ def forward(params, g: Graph, exact: bool = False) -> dict:
         act["xc"].append(xc)
         act["xv"].append(xv)
     act["hc3"], act["hv3"] = hc, hv
-    act["xhat"] = hv @ p[HEAD_X:HEAD_X + 64] + p[HEAD_X + 64]
-    act["yhat"] = hc @ p[HEAD_Y:HEAD_Y + 64] + p[HEAD_Y + 64]
+    act["xhat"] = ar.a(g.base_x) + (hv @ p[HEAD_X:HEAD_X + 64] + p[HEAD_X + 64])
+    act["yhat"] = ar.a(g.base_y) + (hc @ p[HEAD_Y:HEAD_Y + 64] + p[HEAD_Y + 64])
     pooled = np.zeros((g.K, 128), ar.dt)
     for q in range(g.K):
         pooled[q, :64] = hv[g.c0[q]:g.c0[q + 1]].sum(0) / (g.c0[q + 1] - g.c0[q])
@@ -207,14 +235,14 @@ def loss_and_grad(params, g: Graph, exact: bool = False, grad: bool = True):
     ex = a["xhat"] - g.tx
     ey = a["yhat"] - g.ty
     ew = a["rho"] - g.tw
-    lx = np.bincount(g.lp_col, weights=ex ** 2, minlength=K) * inv_n
-    ly = np.bincount(g.lp_row, weights=ey ** 2, minlength=K) * inv_m
+    lx = np.bincount(g.lp_col, weights=ex ** 2, minlength=K) * g.lw_x
+    ly = np.bincount(g.lp_row, weights=ey ** 2, minlength=K) * g.lw_y
     loss = float(np.sum(lx + ly + ew ** 2) / K)
     if not grad:
         return loss, None
     G = np.zeros(COUNT, np.float64)
-    dx = ar.a(2 * ex * inv_n[g.lp_col] / K)
-    dy = ar.a(2 * ey * inv_m[g.lp_row] / K)
+    dx = ar.a(2 * ex * g.lw_x[g.lp_col] / K)
+    dy = ar.a(2 * ey * g.lw_y[g.lp_row] / K)
     drho = ar.a(2 * ew / K)
     hv, hc = a["hv3"], a["hc3"]
     G[HEAD_X:HEAD_X + 64] = dx @ hv
@@ -257,19 +285,19 @@ def loss_and_grad(params, g: Graph, exact: bool = False, grad: bool = True):
 
 
 def init_params(seed: int = 0) -> np.ndarray:
-    """He-uniform weights, zero biases, small heads (a NumPy initialisation
-    for CPU tests; the library seeds its own)."""
+    """He-uniform weights, zero biases, small random heads: a NumPy
+    initialisation for tests (the library's own starts its heads at zero)."""
     rng = np.random.default_rng(seed)
     p = np.zeros(COUNT)
-    p[VIN_W:VIN_B] = rng.uniform(-1, 1, 512) * np.sqrt(6 / 8)
-    p[CIN_W:CIN_B] = rng.uniform(-1, 1, 512) * np.sqrt(6 / 8)
+    p[VIN_W:VIN_B] = rng.uniform(-1, 1, 64 * FEAT) * np.sqrt(6 / FEAT)
+    p[CIN_W:CIN_B] = rng.uniform(-1, 1, 64 * FEAT) * np.sqrt(6 / FEAT)
     for l in range(LAYERS):
         for side in range(2):
             p[layer_w(l, side):layer_b(l, side)] = rng.uniform(-1, 1, DENSE_W) * np.sqrt(6 / 128)
     p[HEAD_X:HEAD_X + 64] = rng.uniform(-0.1, 0.1, 64)
     p[HEAD_Y:HEAD_Y + 64] = rng.uniform(-0.1, 0.1, 64)
     p[HEAD_W:HEAD_W + 128] = rng.uniform(-0.1, 0.1, 128)
-    return p
+    return p   # (non-zero heads, so that every gradient block is exercised)
 
 
 def trace_layout(g: Graph) -> list[tuple[str, tuple]]:

@@ -55,6 +55,12 @@ class CWarmStart(C.Structure):
     _fields_ = [("x", P), ("y", P), ("primal_weight", f64)]
 
 
+class CCertificate(C.Structure):
+    _fields_ = [("objective_value", f64), ("primal_residual", f64), ("bound_violation", f64),
+                ("rel_primal", f64), ("rel_dual", f64), ("rel_gap", f64),
+                ("primal_objective", f64), ("dual_objective", f64), ("kkt", f64)]
+
+
 # (name, restype, argtypes) for every entry point declared in the header.
 SIGNATURES = [
     ("pramaan_version", C.c_char_p, []),
@@ -64,12 +70,15 @@ SIGNATURES = [
     ("pramaan_pdhg_solve_batch", C.c_int, [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CResult)]),
     ("pramaan_pdhg_solve_batch_warm", C.c_int,
      [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CWarmStart), C.POINTER(CResult)]),
+    ("pramaan_certify_batch", C.c_int,
+     [C.POINTER(CLp), i32, C.POINTER(CWarmStart), i32, i32, C.POINTER(CCertificate)]),
     ("pramaan_gnn_num_params", i32, []),
     ("pramaan_gnn_create", C.c_int, [i32, C.c_uint64, C.POINTER(P)]),
     ("pramaan_gnn_destroy", C.c_int, [P]),
     ("pramaan_gnn_get_params", C.c_int, [P, P]),
     ("pramaan_gnn_set_params", C.c_int, [P, P]),
-    ("pramaan_gnn_graph_create", C.c_int, [C.POINTER(CLp), i32, C.POINTER(CWarmStart), i32, C.POINTER(P)]),
+    ("pramaan_gnn_graph_create", C.c_int,
+     [C.POINTER(CLp), i32, C.POINTER(CWarmStart), C.POINTER(CWarmStart), i32, C.POINTER(P)]),
     ("pramaan_gnn_graph_destroy", C.c_int, [P]),
     ("pramaan_gnn_predict", C.c_int, [P, P, P, P, P]),
     ("pramaan_gnn_gradients", C.c_int, [P, P, P, C.POINTER(f64)]),

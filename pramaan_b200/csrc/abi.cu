@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "batch.cuh"
+#include "certificate.cuh"
 #include "gnn.cuh"
 #include "pdhg_engine.cuh"
 
@@ -373,6 +374,20 @@ int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual, do
     });
 }
 
+// ---- certificates --------------------------------------------------------
+
+int pramaan_certify_batch(const pramaan_lp* lps, int32_t count, const pramaan_warm_start* points,
+                          int32_t num_points, int32_t device, pramaan_certificate* out) {
+    return guarded([&] {
+        if (count < 0 || num_points < 0) throw InvalidArgument("count and num_points must be >= 0");
+        if (count == 0 || num_points == 0) return;
+        if (!lps || !points || !out) throw InvalidArgument("lps, points and out must not be NULL");
+        DeviceGuard g(device);
+        CertificateBatch cb(lps, count, device);
+        for (int p = 0; p < num_points; ++p) cb.evaluate(points + size_t(p) * count, out + size_t(p) * count);
+    });
+}
+
 // ---- learned warm start --------------------------------------------------
 
 int32_t pramaan_gnn_num_params(void) { return pb::GnnModel::num_params(); }
@@ -413,8 +428,8 @@ int pramaan_gnn_set_params(pramaan_gnn* net, const float* params) {
     });
 }
 
-int pramaan_gnn_graph_create(const pramaan_lp* lps, int32_t count, const pramaan_warm_start* targets,
-                             int32_t device, pramaan_gnn_graph** out) {
+int pramaan_gnn_graph_create(const pramaan_lp* lps, int32_t count, const pramaan_warm_start* hints,
+                             const pramaan_warm_start* targets, int32_t device, pramaan_gnn_graph** out) {
     return guarded([&] {
         if (!out) throw InvalidArgument("out is NULL");
         *out = nullptr;
@@ -422,7 +437,7 @@ int pramaan_gnn_graph_create(const pramaan_lp* lps, int32_t count, const pramaan
         if (count > 0 && !lps) throw InvalidArgument("lps is NULL");
         DeviceGuard g(device);
         auto h = std::make_unique<pramaan_gnn_graph>();
-        h->graph = std::make_unique<GnnGraph>(lps, count, targets, device);
+        h->graph = std::make_unique<GnnGraph>(lps, count, hints, targets, device);
         *out = h.release();
     });
 }

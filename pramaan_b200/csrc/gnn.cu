@@ -458,19 +458,20 @@ __global__ void dw_reduce_kernel(const float* __restrict__ partial, int blocks, 
 // CUDA-core kernels
 // ---------------------------------------------------------------------------
 // h0[r][o] = bf16(relu(sum_f W[o][f] feat[r][f] + b[o]))
+constexpr int kF = kGnnFeat;
 __global__ void input_layer_kernel(const float* __restrict__ feat, int nodes, const float* __restrict__ w,
                                    bf16* __restrict__ out, int ld) {
-    __shared__ float sw[64 * 8 + 64];
-    for (int t = threadIdx.x; t < 64 * 8 + 64; t += blockDim.x) sw[t] = w[t];
+    __shared__ float sw[64 * kF + 64];
+    for (int t = threadIdx.x; t < 64 * kF + 64; t += blockDim.x) sw[t] = w[t];
     __syncthreads();
     GNN_STRIDE(t, (long long)nodes * 64) {
         const long long r = t >> 6;
         const int o = int(t & 63);
-        const float* f = feat + r * 8;
+        const float* f = feat + r * kF;
         float acc = 0.0f;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc = fmaf(sw[o * 8 + q], f[q], acc);
-        acc += sw[512 + o];
+        for (int q = 0; q < kF; ++q) acc = fmaf(sw[o * kF + q], f[q], acc);
+        acc += sw[64 * kF + o];
         out[r * ld + o] = __float2bfloat16_rn(fmaxf(acc, 0.0f));
     }
 }
@@ -531,9 +532,9 @@ __global__ void aggregate_bwd_kernel(const int* __restrict__ rp, const int* __re
     }
 }
 
-// out[r] = w . h[r] + b (w: 64 rounded weights, then the bias); one warp per node.
+// out[r] = base[r] + (w . h[r] + b) (w: 64 rounded weights, then the bias); one warp per node.
 __global__ void head_kernel(const bf16* __restrict__ h, int nodes, const float* __restrict__ wb,
-                            float* __restrict__ out) {
+                            const float* __restrict__ base, float* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
     for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nodes; r += warps) {
@@ -541,7 +542,7 @@ __global__ void head_kernel(const bf16* __restrict__ h, int nodes, const float* 
         float p = fmaf(wb[2 * lane + 1], __high2float(v), wb[2 * lane] * __low2float(v));
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-        if (lane == 0) out[r] = p + wb[64];
+        if (lane == 0) out[r] = base[r] + (p + wb[64]);
     }
 }
 
@@ -581,15 +582,17 @@ struct BiasGradF {      // dz [r][64] BF16
     const bf16* dz;
     __device__ float operator()(int r, int t) const { return bf(dz[size_t(r) * 64 + t]); }
 };
-struct InLayerGradF {   // dz0 = dh0 masked by h0 > 0; t < 512: dz0[o] f[q] (o = t/8, q = t%8); else dz0[t-512]
+constexpr int kInW = 64 * kF;   // input-layer weights; the 64 biases follow
+constexpr int kWide = kInW + 64; // widest chunk partial
+struct InLayerGradF {   // dz0 = dh0 masked by h0 > 0; t < kInW: dz0[o] f[q] (o = t/9, q = t%9); else dz0[t-kInW]
     const float* dh;
     const bf16* h0;
     int ldh0;
     const float* feat;
     __device__ float operator()(int r, int t) const {
-        const int o = t < 512 ? t >> 3 : t - 512;
+        const int o = t < kInW ? t / kF : t - kInW;
         const float g = bf(h0[size_t(r) * ldh0 + o]) > 0.0f ? dh[size_t(r) * 64 + o] : 0.0f;
-        return t < 512 ? g * feat[size_t(r) * 8 + (t & 7)] : g;
+        return t < kInW ? g * feat[size_t(r) * kF + (t % kF)] : g;
     }
 };
 
@@ -731,7 +734,8 @@ void set_smem_attrs_once() {
 // ---------------------------------------------------------------------------
 // GnnGraph
 // ---------------------------------------------------------------------------
-GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* targets, int dev) {
+GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* hints,
+                   const pramaan_warm_start* targets, int dev) {
     device = dev;
     count = count_;
     has_targets = targets != nullptr;
@@ -845,7 +849,28 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
 
     // features (FP64 arithmetic, stored as FP32)
     auto clip = [](double v) { return std::min(10.0, std::max(-10.0, v)); };
-    std::vector<float> hfv(Nz * 8), hfc(Mz * 8);
+    std::vector<float> hfv(Nz * kF), hfc(Mz * kF), hbx(Nz, 0.0f), hby(Mz, 0.0f);
+    std::vector<char> hint_x(Nz, 0), hint_y(Mz, 0);
+    if (hints) {
+        for (int q = 0; q < K; ++q) {
+            const pramaan_warm_start& h = hints[index[size_t(q)]];
+            const int C = c0[size_t(q)], R = r0[size_t(q)];
+            const int nk = c0[size_t(q) + 1] - C, mk = r0[size_t(q) + 1] - R;
+            const double sa = s_a[size_t(q)], sb = s_b[size_t(q)], sc = s_c[size_t(q)];
+            if (h.x)
+                for (int j = 0; j < nk; ++j) {
+                    if (!std::isfinite(h.x[j])) throw InvalidArgument("gnn graph: hint x must be finite");
+                    hbx[size_t(C + j)] = float(h.x[j] * sa / sb);
+                    hint_x[size_t(C + j)] = 1;
+                }
+            if (h.y)
+                for (int i = 0; i < mk; ++i) {
+                    if (!std::isfinite(h.y[i])) throw InvalidArgument("gnn graph: hint y must be finite");
+                    hby[size_t(R + i)] = float(h.y[i] * sa / sc);
+                    hint_y[size_t(R + i)] = 1;
+                }
+        }
+    }
     for (int j = 0; j < n; ++j) {
         const int q = hlpc[size_t(j)];
         const double sa = s_a[size_t(q)], sb = s_b[size_t(q)], sc = s_c[size_t(q)];
@@ -854,7 +879,7 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
         double absum = 0.0;
         for (int p = htp[size_t(j)]; p < htp[size_t(j) + 1]; ++p) absum += std::fabs(hval[size_t(perm[size_t(p)])]);
         const int deg = deg_c[size_t(j)];
-        float* f = &hfv[size_t(j) * 8];
+        float* f = &hfv[size_t(j) * kF];
         f[0] = float(hcost[size_t(j)] / sc);
         f[1] = fl ? 1.0f : 0.0f;
         f[2] = fu ? 1.0f : 0.0f;
@@ -862,7 +887,8 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
         f[4] = fu ? float(clip(hi * sa / sb)) : 0.0f;
         f[5] = float(std::log1p(double(deg)) / 4.0);
         f[6] = deg > 0 ? float(absum / (sa * deg)) : 0.0f;
-        f[7] = 1.0f;
+        f[7] = hint_x[size_t(j)] ? 1.0f : 0.0f;
+        f[8] = float(clip(double(hbx[size_t(j)])));
     }
     for (int i = 0; i < m; ++i) {
         const int q = hlpr[size_t(i)];
@@ -872,7 +898,7 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
         double absum = 0.0;
         for (int e = hrp[size_t(i)]; e < hrp[size_t(i) + 1]; ++e) absum += std::fabs(hval[size_t(e)]);
         const int deg = hrp[size_t(i) + 1] - hrp[size_t(i)];
-        float* f = &hfc[size_t(i) * 8];
+        float* f = &hfc[size_t(i) * kF];
         f[0] = fl && fu && lo == hi ? 1.0f : 0.0f;
         f[1] = fl ? 1.0f : 0.0f;
         f[2] = fu ? 1.0f : 0.0f;
@@ -880,7 +906,8 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
         f[4] = fu ? float(clip(hi / sb)) : 0.0f;
         f[5] = float(std::log1p(double(deg)) / 4.0);
         f[6] = deg > 0 ? float(absum / (sa * deg)) : 0.0f;
-        f[7] = 1.0f;
+        f[7] = hint_y[size_t(i)] ? 1.0f : 0.0f;
+        f[8] = float(clip(double(hby[size_t(i)])));
     }
 
     // chunk tables
@@ -914,7 +941,7 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
     };
     up(rp, hrp); up(ci, hci); up(tp, htp); up(ti, hti);
     up(coef_r, hcr); up(coef_c, hcc); up(tcoef_r, htr); up(tcoef_c, htc);
-    up(fv, hfv); up(fc, hfc); up(lp_col, hlpc); up(lp_row, hlpr); up(lp_scale, hscale);
+    up(fv, hfv); up(fc, hfc); up(base_x, hbx); up(base_y, hby); up(lp_col, hlpc); up(lp_row, hlpr); up(lp_scale, hscale);
     up(vlo, hvlo); up(vhi, hvhi);
     up(cchunk_begin, cb); up(rchunk_begin, rb); up(cchunk_lp, clp); up(rchunk_lp, rlp);
     up(clp_first, cfirst); up(rlp_first, rfirst); up(inv_n, hinv_n); up(inv_m, hinv_m);
@@ -922,7 +949,7 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
     h_vhi = std::move(hvhi);
 
     if (has_targets) {
-        std::vector<float> htx(Nz), hty(Mz), htw(Kz);
+        std::vector<float> htx(Nz), hty(Mz), htw(Kz), hlx(Kz), hly(Kz);
         for (int q = 0; q < K; ++q) {
             const pramaan_warm_start& t = targets[index[size_t(q)]];
             const int nk = c0[size_t(q) + 1] - c0[size_t(q)], mk = r0[size_t(q) + 1] - r0[size_t(q)];
@@ -933,8 +960,14 @@ GnnGraph::GnnGraph(const pramaan_lp* lps, int count_, const pramaan_warm_start* 
             for (int j = 0; j < nk; ++j) htx[size_t(c0[size_t(q)] + j)] = float(t.x[j] * sa / sb);
             for (int i = 0; i < mk; ++i) hty[size_t(r0[size_t(q)] + i)] = float(t.y[i] * sa / sc);
             htw[size_t(q)] = float(std::log(t.primal_weight / omega_ref[size_t(q)]));
+            // per-LP loss weights: squared errors relative to the mean square of the targets
+            double sx = 0.0, sy = 0.0;
+            for (int j = 0; j < nk; ++j) sx += double(htx[size_t(c0[size_t(q)] + j)]) * htx[size_t(c0[size_t(q)] + j)];
+            for (int i = 0; i < mk; ++i) sy += double(hty[size_t(r0[size_t(q)] + i)]) * hty[size_t(r0[size_t(q)] + i)];
+            hlx[size_t(q)] = float(1.0 / (nk * (sx / nk + kLossFloor)));
+            hly[size_t(q)] = mk > 0 ? float(1.0 / (mk * (sy / mk + kLossFloor))) : 0.0f;
         }
-        up(tx, htx); up(ty, hty); up(tw, htw);
+        up(tx, htx); up(ty, hty); up(tw, htw); up(lw_x, hlx); up(lw_y, hly);
     }
     PB_CUDA_CHECK(cudaStreamSynchronize(st));
 }
@@ -957,23 +990,19 @@ GnnModel::GnnModel(int device, uint64_t seed) : dev_(device) {
     w_.alloc(size_t(2 * kGnnLayers) * 64 * 128);
     wt_.alloc(size_t(2 * kGnnLayers) * 64 * 128);
     status_.alloc(1);
-    // He-uniform weights (fan-in), zero biases
+    // He-uniform weights (fan-in), zero biases and heads
     std::vector<float> h(size_t(np), 0.0f);
     uint64_t s = seed;
     auto fill = [&](int off, int count_, int fan_in) {
         const float a = std::sqrt(6.0f / float(fan_in));
         for (int i = 0; i < count_; ++i) h[size_t(off + i)] = uniform(s, a);
     };
-    fill(GnnParams::kVinW, 64 * 8, 8);
-    fill(GnnParams::kCinW, 64 * 8, 8);
+    fill(GnnParams::kVinW, 64 * kGnnFeat, kGnnFeat);
+    fill(GnnParams::kCinW, 64 * kGnnFeat, kGnnFeat);
     for (int l = 0; l < kGnnLayers; ++l)
         for (int side = 0; side < 2; ++side) fill(GnnParams::layer_w(l, side), 64 * 128, 128);
-    const float head = 0.1f;
-    for (int i = 0; i < 64; ++i) {
-        h[size_t(GnnParams::kHeadX + i)] = uniform(s, head);
-        h[size_t(GnnParams::kHeadY + i)] = uniform(s, head);
-    }
-    for (int i = 0; i < 128; ++i) h[size_t(GnnParams::kHeadW + i)] = uniform(s, head);
+    // the heads start at zero: an untrained network returns the hint (or 0)
+    // and omega_ref, and learns a correction from there
     set_params(h.data());
 }
 
@@ -1038,8 +1067,8 @@ void GnnModel::ensure_workspace(const GnnGraph& g) {
         cap_k_ = k;
     }
     if (chunks > cap_chunks_) {
-        // two ping-pong halves of chunk partials, 576 columns wide
-        part_.alloc(chunks * 576 * 2 + 576);
+        // chunk partials and two ping-pong halves, up to kWide columns wide
+        part_.alloc(chunks * kWide * 2 + kWide);
         cap_chunks_ = chunks;
     }
     if (wpart_.size() == 0) wpart_.alloc(size_t(2 * device_sm_count(dev_)) * 128 * 64);
@@ -1106,10 +1135,11 @@ void GnnModel::forward(const GnnGraph& g) {
         PB_CUDA_CHECK(cudaGetLastError());
     }
     // heads
-    head_kernel<<<grid_for((long long)g.n * 32), kT, 0, st_>>>(hv3_.get(), g.n, pr + GnnParams::kHeadX, xhat_.get());
+    head_kernel<<<grid_for((long long)g.n * 32), kT, 0, st_>>>(hv3_.get(), g.n, pr + GnnParams::kHeadX,
+                                                               g.base_x.get(), xhat_.get());
     if (g.m > 0)
         head_kernel<<<grid_for((long long)g.m * 32), kT, 0, st_>>>(hc3_.get(), g.m, pr + GnnParams::kHeadY,
-                                                                   yhat_.get());
+                                                                   g.base_y.get(), yhat_.get());
     PB_CUDA_CHECK(cudaGetLastError());
     // pooled means per LP, then rho
     float* part = part_.get();
@@ -1136,19 +1166,19 @@ double GnnModel::backward(const GnnGraph& g, bool grad) {
     if (g.K == 0) return 0.0;
     const float* pr = pr_.get();
     float* part = part_.get();
-    float* scratch = part_.get() + cap_chunks_ * 576;
+    float* scratch = part_.get() + cap_chunks_ * kWide;
     float* G = g_.get();
     const float inv_k = 1.0f / float(g.K);
     float* drho = rho_.get() + cap_k_;
     // ---- loss per LP: x and y terms from chunk sums, omega term from rho ----
     std::vector<float> hl(size_t(3) * g.K);
     chunk_kernel<<<std::min(g.cchunks, 148 * 8), 32, 0, st_>>>(SqErrF{xhat_.get(), g.tx.get(), g.lp_col.get(),
-                                                                      g.inv_n.get()},
+                                                                      g.lw_x.get()},
                                                               1, g.cchunk_begin.get(), g.cchunks, part);
     lp_sum_kernel<<<grid_for(g.K), kT, 0, st_>>>(part, 1, g.clp_first.get(), g.K, nullptr, lp_sums_.get(), 1);
     if (g.m > 0) {
         chunk_kernel<<<std::min(g.rchunks, 148 * 8), 32, 0, st_>>>(
-            SqErrF{yhat_.get(), g.ty.get(), g.lp_row.get(), g.inv_m.get()}, 1, g.rchunk_begin.get(), g.rchunks, part);
+            SqErrF{yhat_.get(), g.ty.get(), g.lp_row.get(), g.lw_y.get()}, 1, g.rchunk_begin.get(), g.rchunks, part);
         lp_sum_kernel<<<grid_for(g.K), kT, 0, st_>>>(part, 1, g.rlp_first.get(), g.K, nullptr,
                                                     lp_sums_.get() + cap_k_, 1);
     } else {
@@ -1179,13 +1209,13 @@ double GnnModel::backward(const GnnGraph& g, bool grad) {
     PB_CUDA_CHECK(cudaMemcpyAsync(drho, hdrho.data(), size_t(g.K) * 4, cudaMemcpyHostToDevice, st_));
     float* dxh = dagg_.get();                     // per-node head deltas (scratch)
     float* dyh = dagg_.get() + cap_n_;
-    head_delta_kernel<<<grid_for(g.n), kT, 0, st_>>>(xhat_.get(), g.tx.get(), g.lp_col.get(), g.inv_n.get(), inv_k,
+    head_delta_kernel<<<grid_for(g.n), kT, 0, st_>>>(xhat_.get(), g.tx.get(), g.lp_col.get(), g.lw_x.get(), inv_k,
                                                     g.n, dxh);
     chunk_kernel<<<std::min(g.cchunks, 148 * 8), 96, 0, st_>>>(HeadGradF{hv3_.get(), dxh}, 65, g.cchunk_begin.get(),
                                                               g.cchunks, part);
     ordered_total(part, g.cchunks, 65, scratch, G + GnnParams::kHeadX, st_);
     if (g.m > 0) {
-        head_delta_kernel<<<grid_for(g.m), kT, 0, st_>>>(yhat_.get(), g.ty.get(), g.lp_row.get(), g.inv_m.get(),
+        head_delta_kernel<<<grid_for(g.m), kT, 0, st_>>>(yhat_.get(), g.ty.get(), g.lp_row.get(), g.lw_y.get(),
                                                         inv_k, g.m, dyh);
         chunk_kernel<<<std::min(g.rchunks, 148 * 8), 96, 0, st_>>>(HeadGradF{hc3_.get(), dyh}, 65,
                                                                   g.rchunk_begin.get(), g.rchunks, part);
@@ -1252,13 +1282,13 @@ double GnnModel::backward(const GnnGraph& g, bool grad) {
         }
     }
     // ---- input layers ----
-    chunk_kernel<<<std::min(g.cchunks, 148 * 8), 192, 0, st_>>>(InLayerGradF{dhv_.get(), xv_[0].get(), 128, g.fv.get()},
-                                                               576, g.cchunk_begin.get(), g.cchunks, part);
-    ordered_total(part, g.cchunks, 576, scratch, G + GnnParams::kVinW, st_);
+    chunk_kernel<<<std::min(g.cchunks, 148 * 8), 224, 0, st_>>>(InLayerGradF{dhv_.get(), xv_[0].get(), 128, g.fv.get()},
+                                                               kInW + 64, g.cchunk_begin.get(), g.cchunks, part);
+    ordered_total(part, g.cchunks, kInW + 64, scratch, G + GnnParams::kVinW, st_);
     if (g.m > 0) {
-        chunk_kernel<<<std::min(g.rchunks, 148 * 8), 192, 0, st_>>>(
-            InLayerGradF{dhc_.get(), xc_[0].get(), 128, g.fc.get()}, 576, g.rchunk_begin.get(), g.rchunks, part);
-        ordered_total(part, g.rchunks, 576, scratch, G + GnnParams::kCinW, st_);
+        chunk_kernel<<<std::min(g.rchunks, 148 * 8), 224, 0, st_>>>(
+            InLayerGradF{dhc_.get(), xc_[0].get(), 128, g.fc.get()}, kInW + 64, g.rchunk_begin.get(), g.rchunks, part);
+        ordered_total(part, g.rchunks, kInW + 64, scratch, G + GnnParams::kCinW, st_);
     }
     PB_CUDA_CHECK(cudaGetLastError());
     PB_CUDA_CHECK(cudaMemcpyAsync(&hstatus, status_.get(), 4, cudaMemcpyDeviceToHost, st_));

@@ -9,12 +9,17 @@
 // the finite row bounds), s_c (RMS of the minimisation cost) and the
 // reference weight omega_ref = ||c|| / ||b|| (1 when either is zero).
 //
-// Node features (8 per node, FP32):
+// Node features (9 per node, FP32):
 //   variable j:   c_j/s_c, [l_j finite], [u_j finite], clip(l_j s_a/s_b),
-//                 clip(u_j s_a/s_b), log(1+deg_j)/4, mean|A_.j|/s_a, 1
+//                 clip(u_j s_a/s_b), log(1+deg_j)/4, mean|A_.j|/s_a,
+//                 [hint x given], clip(xh_j s_a/s_b)
 //   constraint i: [l_i == u_i], [l_i finite], [u_i finite], clip(l_i/s_b),
-//                 clip(u_i/s_b), log(1+deg_i)/4, mean|A_i.|/s_a, 1
-// (clip to [-10, 10]; a missing bound gives 0).
+//                 clip(u_i/s_b), log(1+deg_i)/4, mean|A_i.|/s_a,
+//                 [hint y given], clip(yh_i s_a/s_c)
+// (clip to [-10, 10]; a missing bound or hint gives 0).  A hint (xh, yh) is
+// an optional prior guess of the LP's solution given by the caller — for a
+// rolling-horizon stream, the previous window's solution shifted by one
+// period — and the x / y heads predict a correction to it.
 //
 // Network (hidden width 64, BF16 weights and activations, FP32 sums):
 //   h_v0 = relu(W_vin f_v + b_vin)          h_c0 = relu(W_cin f_c + b_cin)
@@ -23,17 +28,21 @@
 //     h_c      = relu(W_c^l [h_c ; agg_c] + b_c^l)          (64 x 128 GEMM)
 //     agg_v[j] = sum_i A_ij / (s_a max(1, deg_j)) h_c[i]     (new h_c)
 //     h_v      = relu(W_v^l [h_v ; agg_v] + b_v^l)
-//   xhat_j = w_x . h_v[j] + b_x,   yhat_i = w_y . h_c[i] + b_y,
+//   xhat_j = xh_j s_a/s_b + w_x . h_v[j] + b_x,
+//   yhat_i = yh_i s_a/s_c + w_y . h_c[i] + b_y   (hint terms 0 without a hint),
 //   rho_k  = w_w . [mean_{j in k} h_v ; mean_{i in k} h_c] + b_w
 //   prediction: x_j = clamp(xhat_j s_b/s_a, l_j, u_j), y_i = yhat_i s_c/s_a,
 //               omega_k = omega_ref_k exp(clamp(rho_k, -10, 10)).
 // Every BF16 rounding point (weights, h, agg, dz) is part of the definition:
 // the NumPy restatement rounds at the same points.
 //
-// Loss against a solved point (x*, y*, omega*):
-//   L = 1/K sum_k [ mean_{j in k} (xhat_j - x*_j s_a/s_b)^2
-//                 + mean_{i in k} (yhat_i - y*_i s_a/s_c)^2
-//                 + (rho_k - log(omega*_k / omega_ref_k))^2 ].
+// Loss against a solved point (x*, y*, omega*), with scaled targets
+// tx_j = x*_j s_a/s_b, ty_i = y*_i s_a/s_c, tw_k = log(omega*_k / omega_ref_k):
+//   L = 1/K sum_k [ sum_{j in k} (xhat_j - tx_j)^2 / (n_k (mean_{j in k} tx_j^2 + d))
+//                 + sum_{i in k} (yhat_i - ty_i)^2 / (m_k (mean_{i in k} ty_i^2 + d))
+//                 + (rho_k - tw_k)^2 ],   d = kLossFloor,
+// i.e. each LP's squared error relative to the size of its own solution, so
+// that LPs with large duals do not dominate.
 //
 // The six 64 x 128 layers run on the tensor cores (tcgen05.mma, operands
 // staged by TMA with the 128-byte swizzle, FP32 accumulators in tensor
@@ -53,16 +62,17 @@
 namespace pb {
 
 constexpr int kGnnHidden = 64;
-constexpr int kGnnFeat = 8;
+constexpr int kGnnFeat = 9;
 constexpr int kGnnLayers = 3;
 constexpr int kGnnChunk = 256;   // nodes per reduction chunk (chunks never straddle two LPs)
+constexpr double kLossFloor = 1e-2;   // added to each LP's mean squared target in the loss weights
 
 // Offsets into the flat FP32 parameter vector.
 struct GnnParams {
-    static constexpr int kVinW = 0;                          // [64][8]
-    static constexpr int kVinB = kVinW + 64 * 8;             // [64]
-    static constexpr int kCinW = kVinB + 64;                 // [64][8]
-    static constexpr int kCinB = kCinW + 64 * 8;             // [64]
+    static constexpr int kVinW = 0;                          // [64][9]
+    static constexpr int kVinB = kVinW + 64 * kGnnFeat;      // [64]
+    static constexpr int kCinW = kVinB + 64;                 // [64][9]
+    static constexpr int kCinB = kCinW + 64 * kGnnFeat;      // [64]
     static constexpr int kLayer0 = kCinB + 64;
     static constexpr int kDenseW = 64 * 128;                 // one layer's W [64 out][128 in]
     static constexpr int kLayerStride = 2 * (kDenseW + 64);  // W_c, b_c, W_v, b_v
@@ -77,7 +87,8 @@ struct GnnParams {
 // A packed batch of LPs prepared for the network (device resident).
 class GnnGraph {
 public:
-    GnnGraph(const pramaan_lp* lps, int count, const pramaan_warm_start* targets, int device);
+    GnnGraph(const pramaan_lp* lps, int count, const pramaan_warm_start* hints, const pramaan_warm_start* targets,
+             int device);
     ~GnnGraph();
     GnnGraph(const GnnGraph&) = delete;
     GnnGraph& operator=(const GnnGraph&) = delete;
@@ -94,12 +105,14 @@ public:
     DevBuf<int> rp, ci, tp, ti;                   // CSR of A and of A^T
     DevBuf<float> coef_r, coef_c;                 // A order: A_ij/(s_a deg_i), A_ij/(s_a deg_j)
     DevBuf<float> tcoef_r, tcoef_c;               // A^T order, the same two coefficients
-    DevBuf<float> fv, fc;                         // node features [n][8], [m][8]
+    DevBuf<float> fv, fc;                         // node features [n][9], [m][9]
+    DevBuf<float> base_x, base_y;                 // scaled hints added to the heads ([n], [m])
     DevBuf<int> lp_col, lp_row;                   // LP of each node
     DevBuf<float> lp_scale;                       // [K][4]: s_a, s_b, s_c, 1/K
     DevBuf<double> vlo, vhi;                      // variable bounds
     std::vector<double> h_vlo, h_vhi;             // host copies (prediction clamp)
     DevBuf<float> tx, ty, tw;                     // scaled targets
+    DevBuf<float> lw_x, lw_y;                     // per-LP loss weights (see the loss)
     // chunk tables: chunk c covers nodes [begin[c], begin[c+1]); lp_first[k]..lp_first[k+1]
     int cchunks = 0, rchunks = 0;
     DevBuf<int> cchunk_begin, rchunk_begin, cchunk_lp, rchunk_lp, clp_first, rlp_first;

@@ -256,3 +256,23 @@ def rolling_horizon_stream(count: int, seed: int = 0, T: int | None = None, P: i
         out.append(rolling_horizon_lp(T, P, demand=demand[:, sl], cost=cost[:, :, sl].reshape(-1),
                                       cap=cap[sl]))
     return out
+
+
+def rolling_horizon_shift(x, y, T: int, P: int):
+    """A window's solution mapped onto the next window of its stream.
+
+    In the layout of ``rolling_horizon_lp`` (variables in three blocks of
+    P*T with index p*T + t; balance rows p*T + t, then T capacity rows) the
+    next window covers periods 1..T of this one: every period moves one slot
+    earlier and the new last period repeats the old last one.  Returns
+    (x', y') as float64 arrays (y' is None when y is None)."""
+    def sh(a, lead):
+        a = np.asarray(a, np.float64).reshape(*lead, T)
+        return np.concatenate([a[..., 1:], a[..., -1:]], axis=-1).ravel()
+
+    xs = sh(x, (3, P))
+    if y is None:
+        return xs, None
+    y = np.asarray(y, np.float64)
+    ys = np.concatenate([sh(y[:P * T], (P,)), sh(y[P * T:], (1,))])
+    return xs, ys

@@ -32,39 +32,53 @@ class WarmStart:
         return WarmStart(np.asarray(r.x, np.float64), np.asarray(r.y, np.float64), float(r.primal_weight))
 
 
-def _warm_array(models, points):
+def _warm_array(models, points, required: bool):
     k = len(models)
     arr = (L.CWarmStart * max(k, 1))()
     keep = []
     for i, w in enumerate(points):
         if w is None:
-            raise ValueError("every LP needs a target point")
-        x = _f64(w.x)
-        y = _f64(w.y) if w.y is not None else np.zeros(0)
-        if len(x) != models[i].numVars() or (models[i].numRows() and len(y) != models[i].numRows()):
-            raise ValueError("target point has the wrong length")
+            if required:
+                raise ValueError("every LP needs a target point")
+            arr[i].x, arr[i].y, arr[i].primal_weight = None, None, 0.0
+            continue
+        if required and w.x is None:
+            raise ValueError("every target needs x")
+        x = None if w.x is None else _f64(w.x)
+        y = None if w.y is None else _f64(w.y)
+        if x is not None and len(x) != models[i].numVars():
+            raise ValueError("point x has the wrong length")
+        if y is not None and len(y) != models[i].numRows():
+            raise ValueError("point y has the wrong length")
         keep.extend([x, y])
-        arr[i].x, arr[i].y, arr[i].primal_weight = _ptr(x), _ptr(y), float(w.primal_weight)
+        arr[i].x, arr[i].y, arr[i].primal_weight = _ptr(x), _ptr(y), float(w.primal_weight or 0.0)
     return arr, keep
 
 
 class GnnGraph:
     """A batch of LPs packed for the network on one device (pramaan_gnn_graph)."""
 
-    def __init__(self, models: list[ModelIR], targets: list[WarmStart] | None = None, device: int = 0):
+    def __init__(self, models: list[ModelIR], targets: list[WarmStart] | None = None, device: int = 0,
+                 hints: list[WarmStart | None] | None = None):
         self.models = list(models)
         self.device = device
         k = len(self.models)
         lps = (L.CLp * max(k, 1))()
         for i, md in enumerate(self.models):
             lps[i] = md.c_struct()
-        tptr, keep = (None, [])
+        tptr, hptr, keep = None, None, []
         if targets is not None:
             if len(targets) != k:
                 raise ValueError("one target per model")
-            tptr, keep = _warm_array(self.models, targets)
+            tptr, kt = _warm_array(self.models, targets, True)
+            keep += kt
+        if hints is not None:
+            if len(hints) != k:
+                raise ValueError("one hint (or None) per model")
+            hptr, kh = _warm_array(self.models, hints, False)
+            keep += kh
         h = C.c_void_p()
-        L.check(L.lib().pramaan_gnn_graph_create(lps, k, tptr, device, C.byref(h)))
+        L.check(L.lib().pramaan_gnn_graph_create(lps, k, hptr, tptr, device, C.byref(h)))
         self.handle = h
         del keep
 
@@ -129,13 +143,14 @@ class WarmStartNet:
         self.params = np.load(path)["params"]
 
     # ---- graphs ----
-    def graph(self, models, targets=None) -> GnnGraph:
-        return GnnGraph(models, targets, self.device)
+    def graph(self, models, targets=None, hints=None) -> GnnGraph:
+        return GnnGraph(models, targets, self.device, hints)
 
     # ---- inference / training ----
-    def predict(self, models_or_graph) -> list[WarmStart | None]:
+    def predict(self, models_or_graph, hints=None) -> list[WarmStart | None]:
         """Predicted starting point of every LP (None for LPs without variables)."""
-        g = models_or_graph if isinstance(models_or_graph, GnnGraph) else self.graph(models_or_graph)
+        g = (models_or_graph if isinstance(models_or_graph, GnnGraph)
+             else self.graph(models_or_graph, hints=hints))
         models = g.models
         k = len(models)
         xs = [np.zeros(md.numVars()) for md in models]
@@ -181,29 +196,73 @@ def training_targets(results: list[SolveResult]) -> list[WarmStart]:
 @dataclass
 class WarmSolveInfo:
     warm_iterations: list[int]
+    choices: list[str]          # per LP: "network", "hint" or "cold" (the certified start)
+    start_kkt: list[float]      # the chosen start's relative KKT error
     fallbacks: int
     predict_s: float
+    certify_s: float
     solve_s: float
     fallback_s: float
 
 
-def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOptions,
-                     fallback_iterations: int | None = None) -> tuple[list[SolveResult], WarmSolveInfo]:
-    """Learned warm start, then cold-start fallback.
+def select_starts(models: list[ModelIR], candidates: dict[str, list], device: int = 0):
+    """The certificate decides: for every LP, the candidate start with the
+    smallest FP64 relative KKT error (max of primal, dual and gap) among
+    ``candidates`` (name -> one point or None per LP), with the cold start
+    always among them.  Returns (starts, names, kkt)."""
+    from .certificate import certify_batch
 
-    The network predicts (x, y, omega) for every LP, the batch is solved from
-    those points, and every LP whose warm solve is not optimal (it hit
-    ``options.max_iterations``) is solved again from the cold start with
-    ``fallback_iterations`` (default: the same limit).  The returned result of
-    each LP is whichever solve reached the tolerance; both are judged by the
-    same relative-KKT criterion."""
+    names = list(candidates) + ["cold"]
+    sets = [candidates[nm] for nm in candidates] + [[None] * len(models)]
+    certs = certify_batch(models, sets, device)
+    starts, chosen, kkt = [], [], []
+    for i in range(len(models)):
+        best = len(names) - 1
+        for p in range(len(names) - 1):
+            if sets[p][i] is not None and certs[p][i].kkt < certs[best][i].kkt:
+                best = p
+        starts.append(sets[best][i])
+        chosen.append(names[best])
+        kkt.append(certs[best][i].kkt)
+    return starts, chosen, kkt
+
+
+def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOptions,
+                     fallback_iterations: int | None = None,
+                     hints: list[WarmStart | None] | None = None,
+                     use_predicted_weight: bool = False) -> tuple[list[SolveResult], WarmSolveInfo]:
+    """Learned warm start, certified, with the cold start as fallback.
+
+    1. The network predicts (x, y, omega) for every LP (refining ``hints``
+       when given, see ``GnnGraph``).
+    2. The certificate decides the start of each LP: the network's point, the
+       hint or the cold start, whichever has the smallest FP64 relative KKT
+       error (``select_starts``).
+    3. The batch is solved from those starts (with the predicted primal
+       weight when ``use_predicted_weight``, else the solver's default).
+    4. Every LP whose solve is not optimal (it hit ``options.max_iterations``)
+       is solved again from the cold start with ``fallback_iterations``
+       (default: the same limit).
+    Every answer is judged by the same relative-KKT criterion as a cold solve."""
     import time
 
     t0 = time.perf_counter()
-    warm = net.predict(models)
+    pred = net.predict(models, hints=hints)
     t1 = time.perf_counter()
-    res = solve_batch(models, options, warm=warm)
+    cands = {"network": pred}
+    if hints is not None:
+        cands["hint"] = list(hints)
+    starts, chosen, kkt = select_starts(models, cands, net.device)
+    warm = []
+    for st, nm, p in zip(starts, chosen, pred):
+        if st is None:
+            warm.append(None)
+        else:
+            w = p.primal_weight if (use_predicted_weight and p is not None) else 0.0
+            warm.append(WarmStart(st.x, st.y, w))
     t2 = time.perf_counter()
+    res = solve_batch(models, options, warm=warm)
+    t3 = time.perf_counter()
     warm_its = [r.iterations for r in res]
     bad = [i for i, r in enumerate(res) if r.status != SolveStatus.kOptimal and models[i].numVars() > 0]
     if bad:
@@ -214,5 +273,5 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
         for i, r in zip(bad, cold):
             if r.status == SolveStatus.kOptimal or res[i].status != SolveStatus.kOptimal:
                 res[i] = r
-    t3 = time.perf_counter()
-    return res, WarmSolveInfo(warm_its, len(bad), t1 - t0, t2 - t1, t3 - t2)
+    t4 = time.perf_counter()
+    return res, WarmSolveInfo(warm_its, chosen, kkt, len(bad), t1 - t0, t2 - t1, t3 - t2, t4 - t3)

@@ -45,7 +45,7 @@ def test_features_by_hand():
     assert g.s_b[0] == pytest.approx(np.sqrt(np.mean(b ** 2)))
     # costs negated for the maximisation
     assert g.fv[0, 0] == pytest.approx(-3.0 / g.s_c[0], rel=1e-6)
-    assert g.fv[:, 7].tolist() == [1.0, 1.0]
+    assert g.fv[:, 7].tolist() == [0.0, 0.0] and g.fv[:, 8].tolist() == [0.0, 0.0]   # no hint
     # x1 appears in two rows: log(3)/4
     assert g.fv[0, 5] == pytest.approx(np.log(3.0) / 4, rel=1e-6)
     # row 2: 3x1 + 2x2 <= 18: mean |A| / s_a
@@ -76,6 +76,31 @@ def test_exact_gradient_matches_finite_differences(seed):
         lm, _ = og.loss_and_grad(p - e, g, exact=True, grad=False)
         fd = (lp - lm) / (2 * h)
         assert grad[i] == pytest.approx(fd, rel=1e-4, abs=1e-7), (int(i), grad[i], fd)
+
+
+def test_hints_enter_features_and_heads():
+    models = [rolling_horizon_lp(3, 2, seed=5), KNOWN["wyndor"][0]]
+    rng = np.random.default_rng(1)
+    hints = [WarmStart(rng.uniform(0, 50, models[0].numVars()), None, 0.0),
+             WarmStart(None, rng.normal(0, 3, 3), 0.0)]
+    g0, g1 = og.Graph(models), og.Graph(models, hints=hints)
+    p = og.init_params(2)
+    a0, a1 = og.forward(p, g0, exact=True), og.forward(p, g1, exact=True)
+    n0 = models[0].numVars()
+    assert g1.fv[:n0, 7].all() and not g1.fv[n0:, 7].any()
+    assert g1.fc[models[0].numRows():, 7].all() and not g1.fc[:models[0].numRows(), 7].any()
+    np.testing.assert_allclose(g1.fv[:n0, 8], np.clip(hints[0].x * g1.s_a[0] / g1.s_b[0], -10, 10), rtol=1e-6)
+    # the heads add the scaled hint to the network's correction
+    assert not np.allclose(a0["xhat"][:n0], a1["xhat"][:n0])
+    # gradients stay exact with hints
+    tg = _targets(models, 3)
+    g2 = og.Graph(models, tg, hints)
+    loss, grad = og.loss_and_grad(p, g2, exact=True)
+    e = np.zeros(og.COUNT)
+    i = og.VIN_W + 8             # the weight of the hint-value feature
+    e[i] = 1e-6
+    fd = (og.loss_and_grad(p + e, g2, exact=True, grad=False)[0] - og.loss_and_grad(p - e, g2, exact=True, grad=False)[0]) / 2e-6
+    assert grad[i] == pytest.approx(fd, rel=1e-4, abs=1e-7)
 
 
 def test_loss_is_zero_at_the_prediction():

@@ -50,6 +50,7 @@ def targets_for(models, seed=0):
 
 def check_trace(models, seed):
     net = WarmStartNet(seed=seed)
+    net.params = og.init_params(seed).astype(np.float32)   # non-zero heads
     p = net.params
     G = net.graph(models)
     tr = split_trace(og.Graph(models), net.trace(G))
@@ -90,6 +91,7 @@ def test_gradients_match_oracle(big):
               else small_models())
     tg = targets_for(models, seed=3)
     net = WarmStartNet(seed=4)
+    net.params = og.init_params(4).astype(np.float32)      # non-zero heads: every block has a gradient
     p = net.params
     loss, grad = net.gradients(net.graph(models, tg))
     oloss, ograd = og.loss_and_grad(p, og.Graph(models, tg), exact=False)
@@ -103,6 +105,7 @@ def test_gradients_are_deterministic():
     models = small_models()
     tg = targets_for(models, seed=5)
     net = WarmStartNet(seed=6)
+    net.params = og.init_params(6).astype(np.float32)
     g = net.graph(models, tg)
     l1, g1 = net.gradients(g)
     l2, g2 = net.gradients(g)
@@ -112,6 +115,8 @@ def test_gradients_are_deterministic():
 def test_params_roundtrip_and_seed():
     a, b = WarmStartNet(seed=11), WarmStartNet(seed=11)
     assert np.array_equal(a.params, b.params)
+    # heads start at zero: the untrained network returns its hint unchanged
+    assert not a.params[og.HEAD_X:].any()
     p = og.init_params(3).astype(np.float32)
     a.params = p
     assert np.array_equal(a.params, p)
@@ -131,6 +136,25 @@ def test_training_fits_solved_targets():
     loss, _ = net.gradients(g)
     oloss, _ = og.loss_and_grad(net.params, og.Graph(models[:4], training_targets(res[:4])), exact=False)
     assert loss == pytest.approx(oloss, rel=1e-3)
+
+
+def test_untrained_network_returns_the_hint():
+    models = small_models()
+    rng = np.random.default_rng(2)
+    hints = [WarmStart(rng.uniform(0, 5, md.numVars()), rng.normal(0, 1, md.numRows()), 0.0) for md in models]
+    net = WarmStartNet(seed=3)
+    pred = net.predict(models, hints=hints)
+    for md, h, p in zip(models, hints, pred):
+        lo, hi = md.var_lower, md.var_upper
+        np.testing.assert_allclose(p.x, np.clip(h.x, lo, hi), rtol=1e-6, atol=1e-6 * np.abs(h.x).max())
+        np.testing.assert_allclose(p.y, h.y, rtol=1e-6, atol=1e-6 * np.abs(h.y).max())
+    # and with hints, the gradients still match the oracle
+    tg = targets_for(models, seed=4)
+    net.params = og.init_params(5).astype(np.float32)
+    loss, grad = net.gradients(net.graph(models, tg, hints))
+    oloss, ograd = og.loss_and_grad(net.params, og.Graph(models, tg, hints), exact=False)
+    assert loss == pytest.approx(oloss, rel=1e-3)
+    assert rel(grad, ograd) < 1e-2
 
 
 def opts(tol=1e-6, it=300000):
@@ -163,3 +187,57 @@ def test_warm_solve_falls_back_to_cold():
     res, info = warm_solve_batch(models, net, opts(it=128), fallback_iterations=300000)
     assert info.fallbacks >= 1
     assert all(r.status == SolveStatus.kOptimal for r in res)
+
+
+def _stream_set(seeds, count, T_range, P_range):
+    from pramaan_b200.generators import rolling_horizon_stream
+    ms, first = [], []
+    for s in seeds:
+        ms += rolling_horizon_stream(count, seed=s, T_range=T_range, P_range=P_range)
+        first += [True] + [False] * (count - 1)
+    return ms, first
+
+
+def _hints(ms, first, res):
+    from pramaan_b200.generators import rolling_horizon_shift
+    out = []
+    for i, md in enumerate(ms):
+        if first[i]:
+            out.append(None)
+            continue
+        PT = md.numVars() // 3
+        T = md.numRows() - PT
+        xs, ys = rolling_horizon_shift(res[i - 1].x, res[i - 1].y, T, PT // T)
+        out.append(WarmStart(xs, ys, 0.0))
+    return out
+
+
+def test_learned_warm_start_saves_iterations_on_a_stream():
+    """Train on solved windows of some streams, then solve held-out streams:
+    the certified learned warm start (network refining the previous window's
+    shifted solution, the certificate choosing each LP's start) needs fewer
+    PDHG iterations in total than cold starts, and every answer meets the
+    tolerance on the FP64 certificate."""
+    from pramaan_b200.certificate import certify_batch
+    o = opts()
+    TR, PR = (24, 48), (5, 10)
+    train, ftr = _stream_set(range(3000, 3080), 5, TR, PR)
+    ev, fev = _stream_set(range(3900, 3903), 12, TR, PR)
+    rtr = solve_batch(train, o)
+    cold = solve_batch(ev, o)
+    assert all(r.status == SolveStatus.kOptimal for r in rtr + cold)
+    htr, hev = _hints(train, ftr, rtr), _hints(ev, fev, cold)
+    idx = [i for i in range(len(train)) if htr[i] is not None]
+    net = WarmStartNet(seed=0)
+    graphs = [net.graph([train[i] for i in idx[k:k + 16]], training_targets([rtr[i] for i in idx[k:k + 16]]),
+                        hints=[htr[i] for i in idx[k:k + 16]]) for k in range(0, len(idx), 16)]
+    net.fit(graphs, epochs=30, lr=1e-3, lr_decay=0.97)
+    res, info = warm_solve_batch(ev, net, o, hints=hev)
+    cold_total = sum(r.iterations for r in cold)
+    warm_total = sum(info.warm_iterations)
+    print(f"learned warm start: {warm_total} iterations vs {cold_total} cold "
+          f"({warm_total / cold_total:.3f}); starts {dict((c, info.choices.count(c)) for c in set(info.choices))}")
+    assert warm_total < 0.9 * cold_total
+    cert = certify_batch(ev, [[WarmStart(r.x, r.y) for r in res]])[0]
+    for r, c in zip(res, cert):
+        assert r.status == SolveStatus.kOptimal and c.kkt <= 1e-6 * 1.0001
