@@ -56,6 +56,12 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--rh-count", type=int, default=128,
+                   help="LPs of the batched rolling-horizon section (the published batch is 512)")
+    p.add_argument("--rh-plain", type=int, default=8, help="LPs of that batch also solved one by one")
+    p.add_argument("--stream-count", type=int, default=32, help="streams of the learned warm-start section")
+    p.add_argument("--stream-windows", type=int, default=6, help="windows per stream in that section")
+    p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
     return p.parse_args()
 
 
@@ -234,6 +240,138 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+def _certified(models, results, tol, device):
+    from pramaan_b200.certificate import certify_batch
+    from pramaan_b200.gnn import WarmStart
+
+    cert = certify_batch(models, [[WarmStart(r.x, r.y) for r in results]], device)[0]
+    return sum(1 for c in cert if c.kkt <= tol * 1.0001)
+
+
+def rolling_horizon_section(args, device):
+    """Batched rolling-horizon LPs (T ~ U{24..336}, P ~ U{5..50}) at 1e-6
+    relative KKT: one packed batch against the same adaptive PDHG solving the
+    LPs one by one (a sample of them)."""
+    from pramaan_b200 import PdhgOptions, PdhgSolver, SolveStatus, solve_batch
+    from pramaan_b200.generators import rolling_horizon_batch
+    from pramaan_b200.pdhg import ALGO_ADAPTIVE
+
+    tol = 1e-6
+    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_ADAPTIVE,
+                    device=device)
+    models = rolling_horizon_batch(args.rh_count, seed=args.seed)
+    solve_batch(models[:2], o)                       # warm-up (module load, occupancy queries)
+    t0 = time.perf_counter()
+    res = solve_batch(models, o)
+    tb = time.perf_counter() - t0
+    its = [r.iterations for r in res]
+    idx = np.linspace(0, len(models) - 1, args.rh_plain).astype(int)
+    solver = PdhgSolver(o)
+    plain_t, plain_it = [], []
+    for i in idx:
+        t0 = time.perf_counter()
+        r = solver.solve(models[i])
+        plain_t.append(time.perf_counter() - t0)
+        plain_it.append(r.iterations)
+    batched = len(models) / tb
+    plain = len(idx) / sum(plain_t)
+    return {"workload": f"rolling_horizon_batch {len(models)} LPs (T~U{{24..336}}, P~U{{5..50}}), "
+                        f"rel KKT {tol:g}, seed {args.seed}",
+            "rows": sum(m.numRows() for m in models), "cols": sum(m.numVars() for m in models),
+            "nnz": sum(m.nnz() for m in models),
+            "batched_lps_per_s": batched, "batched_s": tb, "batched_iterations_median": float(np.median(its)),
+            "optimal": sum(r.status == SolveStatus.kOptimal for r in res),
+            "certified": _certified(models, res, tol, device),
+            "plain_lps_per_s": plain, "plain_sample": int(len(idx)),
+            "plain_time_to_tol_median_s": float(np.median(plain_t)),
+            "plain_iterations_median": float(np.median(plain_it)),
+            "batched_over_plain": batched / plain}
+
+
+def learned_stream_section(args, device):
+    """S streams of rolling-horizon windows solved step by step (window w of
+    every stream is one batch), cold against the certified learned warm start
+    (network refining the previous window's shifted solution) and against the
+    shifted solution alone."""
+    from pramaan_b200 import PdhgOptions, SolveStatus, solve_batch
+    from pramaan_b200.gnn import WarmStartNet, warm_solve_batch
+    from pramaan_b200.pdhg import ALGO_ADAPTIVE
+    from pramaan_b200.train_warm_start import DEFAULT_OUT, stream_windows
+
+    if not DEFAULT_OUT.exists():
+        return {"unavailable": f"no trained weights at {DEFAULT_OUT.name}"}
+    rec = json.loads(str(np.load(DEFAULT_OUT)["record"]))
+    net = WarmStartNet(device=device, seed=0)
+    net.load(DEFAULT_OUT)
+    tol = 1e-6
+    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_ADAPTIVE,
+                    device=device)
+    S, W = args.stream_count, args.stream_windows
+    ms, _ = stream_windows(range(700000 + args.seed, 700000 + args.seed + S), W, tuple(rec["T"]), tuple(rec["P"]))
+    windows = [[ms[s * W + w] for s in range(S)] for w in range(W)]
+    out = {"workload": f"{S} streams x {W} windows (rolling_horizon_stream, T~U{{{rec['T'][0]}..{rec['T'][1]}}}, "
+                       f"P~U{{{rec['P'][0]}..{rec['P'][1]}}}, AR(1) phi 0.9 sigma 0.1), rel KKT {tol:g}; "
+                       "window w of every stream is one batch",
+           "trained_on": {k: rec[k] for k in ("instances_solved", "instances_trained", "epochs")}}
+    solve_batch(windows[0][:2], o)                   # warm-up
+    # the plain per-LP solver on a sample of the same windows
+    from pramaan_b200 import PdhgSolver
+    sample = [windows[w][s] for w in range(W) for s in range(0, S, max(1, S // 2))][:8]
+    solver = PdhgSolver(o)
+    t0 = time.perf_counter()
+    for md in sample:
+        solver.solve(md)
+    out["plain"] = {"lps_per_s": len(sample) / (time.perf_counter() - t0), "sample": len(sample)}
+    for mode in ("cold", "hint", "learned"):
+        prev = None
+        its, t, ok, cert, choices = 0, 0.0, 0, 0, {}
+        for w in range(W):
+            batch = windows[w]
+            hints = None if prev is None else _hints_for(batch, prev)
+            t0 = time.perf_counter()
+            if mode == "cold" or hints is None:
+                res = solve_batch(batch, o)
+            elif mode == "hint":
+                res = solve_batch(batch, o, warm=hints)
+            else:
+                res, info = warm_solve_batch(batch, net, o, hints=hints)
+                for c in info.choices:
+                    choices[c] = choices.get(c, 0) + 1
+            t += time.perf_counter() - t0
+            its += sum(r.iterations for r in res)
+            ok += sum(r.status == SolveStatus.kOptimal for r in res)
+            cert += _certified(batch, res, tol, device)
+            prev = res
+        out[mode] = {"lps_per_s": S * W / t, "seconds": t, "iterations": its, "optimal": ok, "certified": cert}
+        if choices:
+            out[mode]["starts"] = choices
+    for mode in ("hint", "learned"):
+        out[mode]["iterations_vs_cold"] = out[mode]["iterations"] / out["cold"]["iterations"]
+        out[mode]["speedup_vs_cold"] = out[mode]["lps_per_s"] / out["cold"]["lps_per_s"]
+    for mode in ("cold", "hint", "learned"):
+        out[mode]["speedup_vs_plain"] = out[mode]["lps_per_s"] / out["plain"]["lps_per_s"]
+    return out
+
+
+def _hints_for(batch, prev):
+    """Each stream's previous window solution shifted onto its current window."""
+    from pramaan_b200 import SolveStatus
+    from pramaan_b200.generators import rolling_horizon_shift
+    from pramaan_b200.gnn import WarmStart
+
+    out = []
+    for md, r in zip(batch, prev):
+        if r.status != SolveStatus.kOptimal:
+            out.append(None)
+            continue
+        PT = md.numVars() // 3
+        T = md.numRows() - PT
+        xs, ys = rolling_horizon_shift(r.x, r.y, T, PT // T)
+        out.append(WarmStart(xs, ys, 0.0))
+    return out
+
+
+# ---------------------------------------------------------------------------
 def run_gpu_arm(args):
     import torch
 
@@ -338,6 +476,9 @@ def run_gpu_arm(args):
                        "iterations_per_call": args.e2e_iters, "calls": args.e2e_calls,
                        "call_s_median": statistics.median(times)}
 
+    if not args.no_rolling:
+        line["rolling_horizon"] = rolling_horizon_section(args, local)
+        line["learned_stream"] = learned_stream_section(args, local)
     if rank == 0 and not args.no_cpu_baseline:
         v, threads, sample = cpu_baseline(model, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
