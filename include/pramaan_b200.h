@@ -173,6 +173,64 @@ PRAMAAN_API int pramaan_pdhg_solve_batch_warm(const pramaan_lp* lps, int32_t cou
                                               const pramaan_warm_start* warm,
                                               pramaan_solve_result* results);
 
+/* ---- precision ladder ---------------------------------------------------------
+ * The two-rung controller of pramaan::PrecisionLadder
+ * (src/gpu/precision_ladder.cpp:55-181) with a GPU FP64 rung between them:
+ *   rung 1  the reference FP32 PDHG (as PdhgSolver::solve, gpu_* options);
+ *           accepted iff status optimal and both reference residuals (the
+ *           solver's FP64 ComputeFp64Residuals check) are <= residual_threshold
+ *           — exactly the reference's gate;
+ *   rung 2  (refine != 0) the adaptive PDHG with FP64 iterative refinement on
+ *           the GPU to refine_tolerance relative KKT; accepted by the same
+ *           gate on its own reference residuals;
+ *   rung 3  escalation: the caller's CPU FP64 solver (the reference runs
+ *           RevisedSimplex with the GPU x as primal_start_hint); result->x then
+ *           holds that hint (the better GPU point).
+ * With refine == 0 the decisions are the reference's. */
+#define PRAMAAN_LADDER_GPU_FP32 0
+#define PRAMAAN_LADDER_GPU_FP64_REFINED 1
+#define PRAMAAN_LADDER_ESCALATE 2
+/* values of PrecisionLadderResult::EscalationReason (include/pramaan/gpu/precision_ladder.hpp) */
+#define PRAMAAN_ESCALATION_NONE 0
+#define PRAMAAN_ESCALATION_HIGH_PRIMAL_RESIDUAL 1
+#define PRAMAAN_ESCALATION_HIGH_DUAL_RESIDUAL 2
+#define PRAMAAN_ESCALATION_GPU_ITERATION_LIMIT 3
+#define PRAMAAN_ESCALATION_GPU_NUMERICAL_FAILURE 4
+#define PRAMAAN_ESCALATION_GPU_NOT_OPTIMAL 5
+
+typedef struct pramaan_ladder_options {
+    double residual_threshold;       /* T, 1e-6 (Options::residual_threshold)      */
+    int32_t gpu_max_iterations;      /* 100000                                     */
+    int32_t gpu_check_frequency;     /* 100                                        */
+    double gpu_tolerance;            /* 1e-6                                       */
+    int32_t refine;                  /* 1: run rung 2 before escalating            */
+    int32_t refine_max_iterations;   /* 400000                                     */
+    double refine_tolerance;         /* 1e-9 relative KKT                          */
+    int32_t device;                  /* 0                                          */
+    int32_t reserved[3];
+} pramaan_ladder_options;
+
+typedef struct pramaan_ladder_result {
+    int32_t stage;                   /* PRAMAAN_LADDER_*                           */
+    int32_t escalation_reason;       /* rung 1's reason (PRAMAAN_ESCALATION_*)      */
+    int32_t refine_escalation_reason;/* rung 2's reason when it ran                */
+    int32_t gpu_status, gpu_iterations;
+    int32_t refine_status, refine_iterations;
+    int32_t reserved;
+    double gpu_primal_residual, gpu_dual_residual, gpu_objective, gpu_elapsed_ms;
+    double refine_primal_residual, refine_dual_residual, refine_objective, refine_elapsed_ms;
+    double rel_primal, rel_dual, rel_gap;   /* relative KKT of the returned point  */
+    double objective_value;          /* of the returned point, model's sense       */
+    double total_elapsed_ms;
+    double* x;                       /* out [n]: the accepted point / CPU hint      */
+    double* y;                       /* out [m] (may be NULL)                      */
+    double* row_activity;            /* out [m] (may be NULL)                      */
+} pramaan_ladder_result;
+
+PRAMAAN_API void pramaan_ladder_default_options(pramaan_ladder_options* opt);
+PRAMAAN_API int pramaan_ladder_solve(const pramaan_lp* lp, const pramaan_ladder_options* opt,
+                                     pramaan_ladder_result* result);
+
 /* ---- certificates -----------------------------------------------------------
  * FP64 certificate of a point (x, y) of an LP, computed on the GPU.  The first
  * three fields are the reference certificate's (pramaan::generate_certificate,

@@ -102,13 +102,19 @@ def build_reference(force: bool = False) -> dict[str, Path]:
     if force or not _newer(facade_obj, facade):
         jobs.append([*cxx, *inc, "-I", str(REPO / "include"), "-c", str(facade), "-o",
                      str(facade_obj)])
+    # the reference's precision-ladder controller, compiled with its GPU rung enabled
+    ladder_src = REF_SRC / "src" / "gpu" / "precision_ladder.cpp"
+    ladder_obj = obj_dir / "precision_ladder_cuda.o"
+    if force or not _newer(ladder_obj, ladder_src):
+        jobs.append([*cxx, *inc, "-DPRAMAAN_ENABLE_CUDA", "-c", str(ladder_src), "-o", str(ladder_obj)])
     tests = {}
-    for t in ("test_gpu_pdhg", "test_pdhg_kernel"):
+    for t in ("test_gpu_pdhg", "test_pdhg_kernel", "test_precision_ladder"):
         src = REF_SRC / "tests" / f"{t}.cpp"
         obj = obj_dir / f"{t}.o"
         tests[t] = obj
+        extra = ["-DPRAMAAN_ENABLE_CUDA"] if t == "test_precision_ladder" else []
         if force or not _newer(obj, src):
-            jobs.append([*cxx, *inc, "-c", str(src), "-o", str(obj)])
+            jobs.append([*cxx, *inc, *extra, "-c", str(src), "-o", str(obj)])
     with cf.ThreadPoolExecutor(max_workers=8) as ex:
         list(ex.map(_run, jobs))
 
@@ -125,13 +131,17 @@ def build_reference(force: bool = False) -> dict[str, Path]:
     # The reference's GPU test programs, against its own library ...
     for t, obj in tests.items():
         exe = REF_OUT / f"{t}__reference"
-        _run([nvcc, *ARCH, "-o", str(exe), str(obj), *core_objs, *gpu_objs])
+        extra = [str(ladder_obj)] if t == "test_precision_ladder" else []
+        _run([nvcc, *ARCH, "-o", str(exe), str(obj), *extra, *core_objs, *gpu_objs])
         out[f"{t}__reference"] = exe
-    # ... and against libpramaan_b200 through the C++ facade (drop-in check).
+    # ... and against libpramaan_b200 through the C++ facade (drop-in check;
+    # the precision ladder is the reference's own controller calling the
+    # facade's PdhgSolver).
     lib_dir = REPO / "pramaan_b200"
     for t, obj in tests.items():
         exe = REF_OUT / f"{t}__pramaan_b200"
-        _run(["g++", "-o", str(exe), str(obj), str(facade_obj), *core_objs,
+        extra = [str(ladder_obj)] if t == "test_precision_ladder" else []
+        _run(["g++", "-o", str(exe), str(obj), *extra, str(facade_obj), *core_objs,
               f"-L{lib_dir}", "-lpramaan_b200", f"-Wl,-rpath,$ORIGIN/../../pramaan_b200"])
         out[f"{t}__pramaan_b200"] = exe
     # The reference's MPS fixtures, for the programs above (they open

@@ -20,5 +20,7 @@ from .pdhg import (  # noqa: F401
     solve_batch,
 )
 from ._lib import LIB_PATH, PramaanError, lib  # noqa: F401
+from .certificate import Certificate, certify, certify_batch  # noqa: F401
+from .ladder import LadderOptions, PrecisionLadder, PrecisionLadderResult  # noqa: F401
 
 __version__ = "0.1.0"

@@ -55,6 +55,23 @@ class CWarmStart(C.Structure):
     _fields_ = [("x", P), ("y", P), ("primal_weight", f64)]
 
 
+class CLadderOptions(C.Structure):
+    _fields_ = [("residual_threshold", f64), ("gpu_max_iterations", i32), ("gpu_check_frequency", i32),
+                ("gpu_tolerance", f64), ("refine", i32), ("refine_max_iterations", i32),
+                ("refine_tolerance", f64), ("device", i32), ("reserved", i32 * 3)]
+
+
+class CLadderResult(C.Structure):
+    _fields_ = [("stage", i32), ("escalation_reason", i32), ("refine_escalation_reason", i32),
+                ("gpu_status", i32), ("gpu_iterations", i32), ("refine_status", i32),
+                ("refine_iterations", i32), ("reserved", i32),
+                ("gpu_primal_residual", f64), ("gpu_dual_residual", f64), ("gpu_objective", f64),
+                ("gpu_elapsed_ms", f64), ("refine_primal_residual", f64), ("refine_dual_residual", f64),
+                ("refine_objective", f64), ("refine_elapsed_ms", f64), ("rel_primal", f64),
+                ("rel_dual", f64), ("rel_gap", f64), ("objective_value", f64), ("total_elapsed_ms", f64),
+                ("x", P), ("y", P), ("row_activity", P)]
+
+
 class CCertificate(C.Structure):
     _fields_ = [("objective_value", f64), ("primal_residual", f64), ("bound_violation", f64),
                 ("rel_primal", f64), ("rel_dual", f64), ("rel_gap", f64),
@@ -70,6 +87,8 @@ SIGNATURES = [
     ("pramaan_pdhg_solve_batch", C.c_int, [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CResult)]),
     ("pramaan_pdhg_solve_batch_warm", C.c_int,
      [C.POINTER(CLp), i32, C.POINTER(COptions), C.POINTER(CWarmStart), C.POINTER(CResult)]),
+    ("pramaan_ladder_default_options", None, [C.POINTER(CLadderOptions)]),
+    ("pramaan_ladder_solve", C.c_int, [C.POINTER(CLp), C.POINTER(CLadderOptions), C.POINTER(CLadderResult)]),
     ("pramaan_certify_batch", C.c_int,
      [C.POINTER(CLp), i32, C.POINTER(CWarmStart), i32, i32, C.POINTER(CCertificate)]),
     ("pramaan_gnn_num_params", i32, []),

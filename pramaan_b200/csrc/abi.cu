@@ -153,6 +153,15 @@ pramaan_pdhg_options defaults() {
     return o;
 }
 
+// Re-raises the failure of a nested entry point with its own text.
+[[noreturn]] void throw_last(int rc) {
+    const std::string msg = g_last_error;
+    if (rc == PRAMAAN_ERR_INVALID_ARGUMENT) throw InvalidArgument(msg);
+    if (rc == PRAMAAN_ERR_DEVICE_TIMEOUT) throw DeviceTimeout(msg);
+    if (rc == PRAMAAN_ERR_CUDA) throw CudaError(msg);
+    throw std::runtime_error(msg);
+}
+
 void same_device(const pramaan_gnn* net, const pramaan_gnn_graph* gr) {
     if (!net || !gr) throw InvalidArgument("net and graph must not be NULL");
     if (net->device != gr->graph->device) throw InvalidArgument("net and graph live on different devices");
@@ -371,6 +380,114 @@ int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual, do
         if (!s) throw InvalidArgument("session is NULL");
         if (bytes_dual) *bytes_dual = s->eng->bytes_dual();
         if (bytes_primal) *bytes_primal = s->eng->bytes_primal();
+    });
+}
+
+// ---- precision ladder ----------------------------------------------------
+
+void pramaan_ladder_default_options(pramaan_ladder_options* opt) {
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->residual_threshold = 1e-6;
+    opt->gpu_max_iterations = 100000;
+    opt->gpu_check_frequency = 100;
+    opt->gpu_tolerance = 1e-6;
+    opt->refine = 1;
+    opt->refine_max_iterations = 400000;
+    opt->refine_tolerance = 1e-9;
+    opt->device = 0;
+}
+
+namespace {
+// The reference gate (src/gpu/precision_ladder.cpp:91-121): accept iff
+// optimal and both residuals <= T; otherwise the escalation reason.
+int ladder_gate(const pramaan_solve_result& r, double T) {
+    if (r.status == PRAMAAN_STATUS_OPTIMAL) {
+        if (r.primal_residual <= T && r.dual_residual <= T) return PRAMAAN_ESCALATION_NONE;
+        return r.primal_residual > T ? PRAMAAN_ESCALATION_HIGH_PRIMAL_RESIDUAL : PRAMAAN_ESCALATION_HIGH_DUAL_RESIDUAL;
+    }
+    if (r.status == PRAMAAN_STATUS_ITERATION_LIMIT) return PRAMAAN_ESCALATION_GPU_ITERATION_LIMIT;
+    if (r.status == PRAMAAN_STATUS_NUMERICAL_FAILURE) return PRAMAAN_ESCALATION_GPU_NUMERICAL_FAILURE;
+    return PRAMAAN_ESCALATION_GPU_NOT_OPTIMAL;
+}
+}  // namespace
+
+int pramaan_ladder_solve(const pramaan_lp* lp, const pramaan_ladder_options* opt, pramaan_ladder_result* out) {
+    return guarded([&] {
+        if (!lp || !out) throw InvalidArgument("lp and result must not be NULL");
+        pramaan_ladder_options o;
+        pramaan_ladder_default_options(&o);
+        if (opt) o = *opt;
+        const auto t0 = std::chrono::steady_clock::now();
+        const int n = lp->num_cols, m = lp->num_rows;
+        std::vector<double> x1(size_t(n > 0 ? n : 1)), y1(size_t(m > 0 ? m : 1)), a1(size_t(m > 0 ? m : 1));
+        // ---- rung 1: the reference FP32 PDHG ----
+        pramaan_pdhg_options g = defaults();
+        g.tolerance = o.gpu_tolerance;
+        g.max_iterations = o.gpu_max_iterations;
+        g.check_frequency = o.gpu_check_frequency;
+        g.device = o.device;
+        pramaan_solve_result r1{};
+        r1.x = x1.data(); r1.y = y1.data(); r1.row_activity = a1.data();
+        const int rc1 = pramaan_pdhg_solve(lp, &g, &r1);
+        if (rc1 != PRAMAAN_OK) throw_last(rc1);
+        out->gpu_status = r1.status;
+        out->gpu_iterations = r1.iterations;
+        out->gpu_primal_residual = r1.primal_residual;
+        out->gpu_dual_residual = r1.dual_residual;
+        out->gpu_objective = r1.objective_value;
+        out->gpu_elapsed_ms = r1.solve_ms;
+        out->escalation_reason = ladder_gate(r1, o.residual_threshold);
+        out->refine_escalation_reason = PRAMAAN_ESCALATION_NONE;
+        out->refine_status = PRAMAAN_STATUS_ITERATION_LIMIT;
+        out->refine_iterations = 0;
+        out->refine_primal_residual = out->refine_dual_residual = std::numeric_limits<double>::infinity();
+        out->refine_objective = 0.0;
+        out->refine_elapsed_ms = 0.0;
+        const pramaan_solve_result* best = &r1;
+        pramaan_solve_result r2{};
+        std::vector<double> x2, y2, a2;
+        if (out->escalation_reason == PRAMAAN_ESCALATION_NONE) {
+            out->stage = PRAMAAN_LADDER_GPU_FP32;
+        } else if (o.refine) {
+            // ---- rung 2: FP64 refinement on the GPU ----
+            x2.resize(x1.size()); y2.resize(y1.size()); a2.resize(a1.size());
+            pramaan_pdhg_options g2 = defaults();
+            g2.algorithm = PRAMAAN_ALGO_ADAPTIVE;
+            g2.termination = PRAMAAN_TERM_RELATIVE_KKT;
+            g2.refine = 1;
+            g2.tolerance = o.refine_tolerance;
+            g2.max_iterations = o.refine_max_iterations;
+            g2.check_frequency = 64;
+            g2.device = o.device;
+            r2.x = x2.data(); r2.y = y2.data(); r2.row_activity = a2.data();
+            const int rc2 = pramaan_pdhg_solve(lp, &g2, &r2);
+            if (rc2 != PRAMAAN_OK) throw_last(rc2);
+            out->refine_status = r2.status;
+            out->refine_iterations = r2.iterations;
+            out->refine_primal_residual = r2.primal_residual;
+            out->refine_dual_residual = r2.dual_residual;
+            out->refine_objective = r2.objective_value;
+            out->refine_elapsed_ms = r2.solve_ms;
+            out->refine_escalation_reason = ladder_gate(r2, o.residual_threshold);
+            const bool better = r2.status == PRAMAAN_STATUS_OPTIMAL &&
+                                std::max(r2.primal_residual, r2.dual_residual) <=
+                                    std::max(r1.primal_residual, r1.dual_residual);
+            if (out->refine_escalation_reason == PRAMAAN_ESCALATION_NONE || better) best = &r2;
+            out->stage = out->refine_escalation_reason == PRAMAAN_ESCALATION_NONE ? PRAMAAN_LADDER_GPU_FP64_REFINED
+                                                                                : PRAMAAN_LADDER_ESCALATE;
+        } else {
+            out->stage = PRAMAAN_LADDER_ESCALATE;
+        }
+        out->rel_primal = best->rel_primal;
+        out->rel_dual = best->rel_dual;
+        out->rel_gap = best->rel_gap;
+        out->objective_value = best->objective_value;
+        if (out->x && n > 0) std::memcpy(out->x, best->x, size_t(n) * 8);
+        if (out->y && m > 0) std::memcpy(out->y, best->y, size_t(m) * 8);
+        if (out->row_activity && m > 0) std::memcpy(out->row_activity, best->row_activity, size_t(m) * 8);
+        out->total_elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     });
 }
 

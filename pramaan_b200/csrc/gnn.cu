@@ -584,17 +584,31 @@ struct BiasGradF {      // dz [r][64] BF16
 };
 constexpr int kInW = 64 * kF;   // input-layer weights; the 64 biases follow
 constexpr int kWide = kInW + 64; // widest chunk partial
-struct InLayerGradF {   // dz0 = dh0 masked by h0 > 0; t < kInW: dz0[o] f[q] (o = t/9, q = t%9); else dz0[t-kInW]
-    const float* dh;
-    const bf16* h0;
-    int ldh0;
-    const float* feat;
-    __device__ float operator()(int r, int t) const {
-        const int o = t < kInW ? t / kF : t - kInW;
-        const float g = bf(h0[size_t(r) * ldh0 + o]) > 0.0f ? dh[size_t(r) * 64 + o] : 0.0f;
-        return t < kInW ? g * feat[size_t(r) * kF + (t % kF)] : g;
+
+// Input-layer gradient partials: part[c][o*9 + q] = sum_{r in chunk c} dz0[r][o] f[r][q],
+// part[c][kInW + o] = sum_r dz0[r][o], with dz0 = dh0 masked by h0 > 0.  One
+// thread per output feature o (coalesced dh / h0 reads), nodes in order.
+__global__ void inlayer_grad_kernel(const float* __restrict__ dh, const bf16* __restrict__ h0, int ldh0,
+                                    const float* __restrict__ feat, const int* __restrict__ begin, int chunks,
+                                    float* __restrict__ part) {
+    const int o = threadIdx.x;   // blockDim.x == 64
+    for (int c = blockIdx.x; c < chunks; c += gridDim.x) {
+        float acc[kF + 1];
+#pragma unroll
+        for (int q = 0; q <= kF; ++q) acc[q] = 0.0f;
+        for (int r = begin[c]; r < begin[c + 1]; ++r) {
+            const float g = bf(h0[size_t(r) * ldh0 + o]) > 0.0f ? dh[size_t(r) * 64 + o] : 0.0f;
+            const float* f = feat + size_t(r) * kF;
+#pragma unroll
+            for (int q = 0; q < kF; ++q) acc[q] += g * f[q];
+            acc[kF] += g;
+        }
+        float* dst = part + size_t(c) * kWide;
+#pragma unroll
+        for (int q = 0; q < kF; ++q) dst[o * kF + q] = acc[q];
+        dst[kInW + o] = acc[kF];
     }
-};
+}
 
 // out[k][t] = scale_k * sum_{c in LP k's chunks} part[c][t]
 __global__ void lp_sum_kernel(const float* __restrict__ part, int width, const int* __restrict__ lp_first, int K,
@@ -1282,13 +1296,13 @@ double GnnModel::backward(const GnnGraph& g, bool grad) {
         }
     }
     // ---- input layers ----
-    chunk_kernel<<<std::min(g.cchunks, 148 * 8), 224, 0, st_>>>(InLayerGradF{dhv_.get(), xv_[0].get(), 128, g.fv.get()},
-                                                               kInW + 64, g.cchunk_begin.get(), g.cchunks, part);
-    ordered_total(part, g.cchunks, kInW + 64, scratch, G + GnnParams::kVinW, st_);
+    inlayer_grad_kernel<<<std::min(g.cchunks, 148 * 16), 64, 0, st_>>>(dhv_.get(), xv_[0].get(), 128, g.fv.get(),
+                                                                         g.cchunk_begin.get(), g.cchunks, part);
+    ordered_total(part, g.cchunks, kWide, scratch, G + GnnParams::kVinW, st_);
     if (g.m > 0) {
-        chunk_kernel<<<std::min(g.rchunks, 148 * 8), 224, 0, st_>>>(
-            InLayerGradF{dhc_.get(), xc_[0].get(), 128, g.fc.get()}, kInW + 64, g.rchunk_begin.get(), g.rchunks, part);
-        ordered_total(part, g.rchunks, kInW + 64, scratch, G + GnnParams::kCinW, st_);
+        inlayer_grad_kernel<<<std::min(g.rchunks, 148 * 16), 64, 0, st_>>>(dhc_.get(), xc_[0].get(), 128, g.fc.get(),
+                                                                           g.rchunk_begin.get(), g.rchunks, part);
+        ordered_total(part, g.rchunks, kWide, scratch, G + GnnParams::kCinW, st_);
     }
     PB_CUDA_CHECK(cudaGetLastError());
     PB_CUDA_CHECK(cudaMemcpyAsync(&hstatus, status_.get(), 4, cudaMemcpyDeviceToHost, st_));

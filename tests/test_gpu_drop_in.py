@@ -1,6 +1,8 @@
 """Drop-in check: the reference's own GPU test programs
-(tests/test_gpu_pdhg.cpp, tests/test_pdhg_kernel.cpp), compiled unmodified
-from its sources and linked against libpramaan_b200 through the C++ facade
+(tests/test_gpu_pdhg.cpp, tests/test_pdhg_kernel.cpp and
+tests/test_precision_ladder.cpp with the reference's own controller
+src/gpu/precision_ladder.cpp), compiled unmodified from its sources and linked
+against libpramaan_b200 through the C++ facade
 (pramaan_b200/csrc/facade/pdhg_solver.cpp), must pass.  The same programs
 linked against the reference's own GPU library are run beside them.
 
@@ -24,13 +26,13 @@ def run(exe: str):
     return r.returncode, r.stdout + r.stderr
 
 
-@pytest.mark.parametrize("prog", ["test_gpu_pdhg", "test_pdhg_kernel"])
+@pytest.mark.parametrize("prog", ["test_gpu_pdhg", "test_pdhg_kernel", "test_precision_ladder"])
 def test_reference_program_passes_on_pramaan_b200(prog):
     rc, out = run(f"{prog}__pramaan_b200")
     assert rc == 0 and "TEST SUITE PASSED" in out, out[-4000:]
 
 
-@pytest.mark.parametrize("prog", ["test_gpu_pdhg", "test_pdhg_kernel"])
+@pytest.mark.parametrize("prog", ["test_gpu_pdhg", "test_pdhg_kernel", "test_precision_ladder"])
 def test_reference_program_on_reference_library(prog):
     rc, out = run(f"{prog}__reference")
     print(out[-3000:])
