@@ -56,6 +56,12 @@ extern "C" {
 #define PRAMAAN_ALGO_ADAPTIVE 1  /* same iteration with Ruiz + Pock-Chambolle steps, primal
                                     weight, averaging and KKT-based adaptive restarts;
                                     needs PRAMAAN_TERM_RELATIVE_KKT */
+#define PRAMAAN_ALGO_HALPERN 2   /* restarted Halpern PDHG with reflection: the same
+                                    preconditioned steps and primal weight, each
+                                    iterate moved to w((1+r)T(z) - r z) + (1-w) z0
+                                    (w = (k+1)/(k+2), r = 1, z0 the restart point),
+                                    restarts on the fixed-point residual; needs
+                                    PRAMAAN_TERM_RELATIVE_KKT and refine = 1 */
 #define PRAMAAN_TERM_REFERENCE 0 /* abs. max primal violation, rel. max dual violation */
 #define PRAMAAN_TERM_RELATIVE_KKT 1 /* relative primal, dual residual and gap (L2, FP64) */
 
@@ -141,8 +147,9 @@ PRAMAAN_API int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_opti
  * packed into one block-diagonal operand, so each half-iteration of all of
  * them is one kernel launch; each LP keeps its own step size, primal weight,
  * restarts, FP64 refinement and termination, and is frozen once it meets the
- * tolerance.  opt->algorithm must be PRAMAAN_ALGO_ADAPTIVE with
- * PRAMAAN_TERM_RELATIVE_KKT (NULL: the defaults with those two set).
+ * tolerance.  opt->algorithm must be PRAMAAN_ALGO_ADAPTIVE or
+ * PRAMAAN_ALGO_HALPERN with PRAMAAN_TERM_RELATIVE_KKT (NULL: the defaults with
+ * PRAMAAN_ALGO_HALPERN and PRAMAAN_TERM_RELATIVE_KKT).
  * results[k] is LP k's result, with caller-owned x / y / row_activity
  * buffers as in pramaan_pdhg_solve; solve_ms is the whole batch's time.
  * LPs without variables or with non-finite costs get the reference's early

@@ -180,3 +180,75 @@ def solve(model, tol=1e-6, max_iterations=100000, check_frequency=64, return_tra
     if return_trace:
         out["trace"] = trace
     return out
+
+
+def solve_halpern(model, tol=1e-6, max_iterations=100000, check_frequency=64, rho=1.0):
+    """The library's PRAMAAN_ALGO_HALPERN mode restated in FP64.
+
+    Same preconditioned steps, step size and initial primal weight as
+    ``solve``; the PDHG operator taken primal first,
+        x+ = clip(x - t (c + A^T y)),  y+ = dual step of y with A (2 x+ - x),
+    each iteration moving to w ((1 + rho) T(z) - rho z) + (1 - w) z_anchor with
+    w = (k + 1) / (k + 2), k the iterations since the last restart (restarted
+    Halpern PDHG with reflection, Lu and Yang 2024).  At every check
+    (``check_frequency`` iterations) the fixed-point residual
+    r = sqrt(sum (dx)^2 / t + sum (dy)^2 / s) of the interval's first and last
+    iteration is known; an LP restarts at its current iterate when r_last <=
+    0.2 r0, or r_last <= 0.8 r0 and r_last grew since the previous check, or
+    0.36 of all iterations passed since its last restart (r0: the residual
+    of the first iteration after the restart); the primal weight is updated
+    at restarts as in ``solve``; termination on the relative KKT of the
+    current iterate."""
+    P = problem(model)
+    A, AT, c = P["A"], P["AT"], P["c"]
+    m, n = A.shape
+    R, C, sigma, tau = steps(P)
+    eta = 0.99 / op_norm(P, sigma, tau)
+    rl, ru, vl, vu = P["rl"], P["ru"], P["vl"], P["vu"]
+    omega = initial_weight(P, R, C)
+    x = np.clip(0.0, vl, vu) * np.ones(n)
+    y = np.zeros(m)
+    xa, ya = x.copy(), y.copy()
+    k = rel_kkt(P, x, y)
+    it, restarts, last_restart, kk = 0, 0, 0, 0
+    r0, rprev, need_r0 = 0.0, np.inf, True
+    status = "iteration_limit"
+    if k["rel_p"] <= tol and k["rel_d"] <= tol and k["rel_gap"] <= tol:
+        status = "optimal"
+    while status != "optimal" and it < max_iterations:
+        s, t = sigma * eta * omega, tau * eta / omega
+        chunk = min(check_frequency, max_iterations - it)
+        r_first = r_last = 0.0
+        for j in range(chunk):
+            xt = np.clip(x - t * (c + AT @ y), vl, vu)
+            w_ = y / s + A @ (2 * xt - x)
+            yt = s * (w_ - np.clip(w_, rl, ru))
+            r = np.sqrt(np.sum((x - xt) ** 2 / t) + np.sum((y - yt) ** 2 / s))
+            if j == 0:
+                r_first = r
+            if j == chunk - 1:
+                r_last = r
+            wgt = (kk + 1) / (kk + 2)
+            x = wgt * ((1 + rho) * xt - rho * x) + (1 - wgt) * xa
+            y = wgt * ((1 + rho) * yt - rho * y) + (1 - wgt) * ya
+            kk += 1
+            it += 1
+        if need_r0:
+            r0, need_r0 = r_first, False
+        k = rel_kkt(P, x, y)
+        if k["rel_p"] <= tol and k["rel_d"] <= tol and k["rel_gap"] <= tol:
+            status = "optimal"
+            break
+        restart = (r_last <= 0.2 * r0 or (r_last <= 0.8 * r0 and r_last > rprev)
+                   or (it - last_restart) >= 0.36 * it)
+        rprev = r_last
+        if restart:
+            dx = np.linalg.norm((x - xa) / C)
+            dy = np.linalg.norm((y - ya) / R) if m else 0.0
+            if dx > 1e-10 and dy > 1e-10:
+                omega = float(np.exp(0.5 * np.log(dy / dx) + 0.5 * np.log(omega)))
+            xa, ya = x.copy(), y.copy()
+            kk, last_restart, restarts = 0, it, restarts + 1
+            rprev, need_r0 = np.inf, True
+    return dict(status=status, iterations=it, x=x, y=y, restarts=restarts, omega=omega, eta=eta,
+                kkt=rel_kkt(P, x, y))

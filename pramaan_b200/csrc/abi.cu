@@ -194,7 +194,7 @@ int pramaan_pdhg_solve_batch_warm(const pramaan_lp* lps, int32_t count, const pr
         if (count > 0 && (!lps || !results)) throw InvalidArgument("lps and results must not be NULL");
         pramaan_pdhg_options o = opt ? *opt : defaults();
         if (!opt) {
-            o.algorithm = PRAMAAN_ALGO_ADAPTIVE;
+            o.algorithm = PRAMAAN_ALGO_HALPERN;
             o.termination = PRAMAAN_TERM_RELATIVE_KKT;
         }
         DeviceGuard g(o.device);
@@ -238,8 +238,15 @@ int pramaan_pdhg_solve(const pramaan_lp* lp, const pramaan_pdhg_options* opt,
             }
         }
         DeviceGuard g(o.device);
-        PdhgEngine eng(*lp, o);
-        eng.solve(*lp, res);
+        if (o.algorithm == PRAMAAN_ALGO_HALPERN) {
+            // the Halpern iteration lives in the batched engine: a batch of one
+            AdaptiveBatch one(lp, 1, o);
+            one.solve(lp, res);
+            res->compactions = 0.0;
+        } else {
+            PdhgEngine eng(*lp, o);
+            eng.solve(*lp, res);
+        }
         res->solve_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     });

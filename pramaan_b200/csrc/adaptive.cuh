@@ -132,6 +132,110 @@ struct EpiPrimalAdapt {
     __device__ void finish(State&, int) const {}
 };
 
+// ---- restarted Halpern PDHG with reflection -------------------------------
+// The PDHG operator T is taken primal first,
+//   x+ = clip(x - tau (c + A^T y), l_x, u_x),   y+ = dual step of y with A (2 x+ - x),
+// and each iteration moves to the Halpern point with reflection rho = 1:
+//   z <- w ((1 + rho) T(z) - rho z) + (1 - w) z_anchor,   w = (k + 1) / (k + 2),
+// k = iterations since the LP's last restart (Lu and Yang, "Restarted Halpern
+// PDHG for linear programming", 2024).  On FP32 corrections around FP64
+// master iterates the anchor (the restart point) is the master itself, so the
+// anchor term vanishes (anchor == nullptr).  The fixed-point residual
+// ||z - T(z)||^2 in the step-weighted norm (sum (dx)^2/tau + (dy)^2/sigma) is
+// written per element on the iterations that ask for it (fpr != nullptr).
+constexpr float kHalpernReflection = 1.0f;
+
+__device__ __forceinline__ float halpern_weight(const int* iter_base, int offset, const int* restart_iter,
+                                                const int* lp, int i) {
+    const long long k = (long long)(*iter_base) + offset - restart_iter[lp[i]];
+    return k <= 0 ? 0.5f : float(double(k + 1) / double(k + 2));
+}
+
+struct EpiPrimalHalpern {
+    const float* __restrict__ tau;
+    const float* __restrict__ c;
+    const float* __restrict__ l_x;
+    const float* __restrict__ u_x;
+    float* __restrict__ x;
+    float* __restrict__ x_bar;
+    const float* __restrict__ anchor;      // nullptr: 0
+    const int* __restrict__ lp;
+    const int* __restrict__ restart_iter;
+    const int* __restrict__ iter_base;
+    int offset;
+    double* __restrict__ fpr;              // nullptr: not this iteration
+    using State = NoState;
+    __device__ void init(State&) const {}
+    __device__ void prefetch(int j) const {
+        prefetch_l2(tau + j); prefetch_l2(c + j); prefetch_l2(l_x + j); prefetch_l2(u_x + j);
+        prefetch_l2(x + j); prefetch_l2(lp + j);
+    }
+    __device__ void apply(State&, int j, float aty) const {
+        const float x_prev = x[j];
+        const float t = tau[j];
+        if (!(t > 0.0f)) {           // a frozen LP keeps its iterate
+            x_bar[j] = x_prev;
+            if (fpr) fpr[j] = 0.0;
+            return;
+        }
+        const float g = __fadd_rn(c[j], aty);
+        const float xt = fminf(fmaxf(__fmaf_rn(-t, g, x_prev), l_x[j]), u_x[j]);
+        x_bar[j] = __fmaf_rn(2.0f, xt, -x_prev);
+        const float w = halpern_weight(iter_base, offset, restart_iter, lp, j);
+        const float refl = __fmaf_rn(1.0f + kHalpernReflection, xt, -kHalpernReflection * x_prev);
+        const float a = anchor ? anchor[j] : 0.0f;
+        x[j] = __fmaf_rn(w, __fsub_rn(refl, a), a);
+        if (fpr) {
+            const double d = double(x_prev) - double(xt);
+            fpr[j] = d * d / double(t);
+        }
+    }
+    __device__ void finish(State&, int) const {}
+};
+
+struct EpiDualHalpern {
+    const float* __restrict__ sigma;
+    const float* __restrict__ r_lo;
+    const float* __restrict__ r_hi;
+    const float* __restrict__ y_m;         // FP32 copy of the master dual
+    float* __restrict__ e;
+    const float* __restrict__ anchor;      // nullptr: 0
+    const int* __restrict__ lp;
+    const int* __restrict__ restart_iter;
+    const int* __restrict__ iter_base;
+    int offset;
+    double* __restrict__ fpr;
+    using State = NoState;
+    __device__ void init(State&) const {}
+    __device__ void prefetch(int i) const {
+        prefetch_l2(sigma + i); prefetch_l2(r_lo + i); prefetch_l2(r_hi + i); prefetch_l2(y_m + i);
+        prefetch_l2(e + i); prefetch_l2(lp + i);
+    }
+    __device__ void apply(State&, int i, float ad) const {
+        const float s = sigma[i];
+        const float e_prev = e[i];
+        float en = e_prev;
+        if (s > 0.0f) {
+            const float ym = y_m[i];
+            const float q = __fdiv_rn(__fadd_rn(ym, e_prev), s);
+            const float hi = __fadd_rn(ad, r_hi[i]);
+            const float lo = __fadd_rn(ad, r_lo[i]);
+            if (__fadd_rn(q, hi) > 0.0f) en = __fmaf_rn(s, hi, e_prev);
+            else if (__fadd_rn(q, lo) < 0.0f) en = __fmaf_rn(s, lo, e_prev);
+            else en = -ym;
+        }
+        const float w = halpern_weight(iter_base, offset, restart_iter, lp, i);
+        const float refl = __fmaf_rn(1.0f + kHalpernReflection, en, -kHalpernReflection * e_prev);
+        const float a = anchor ? anchor[i] : 0.0f;
+        e[i] = __fmaf_rn(w, __fsub_rn(refl, a), a);
+        if (fpr) {
+            const double d = double(e_prev) - double(en);
+            fpr[i] = s > 0.0f ? d * d / double(s) : 0.0;
+        }
+    }
+    __device__ void finish(State&, int) const {}
+};
+
 // Row part of the relative KKT error (FP64, on the original problem in
 // minimisation form; lambda = -y since y is the reference's negated
 // multiplier) of x = x_m + d, y = y_m + e: the SpMV delivers (A d)_i, the

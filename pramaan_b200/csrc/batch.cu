@@ -287,6 +287,8 @@ __global__ void scatter_answers_kernel(const int* __restrict__ lp, const int* __
     }
 }
 
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
 template <typename T>
 void regather(DevBuf<T>& b, const DevBuf<int>& map, int len, cudaStream_t st) {
     if (b.size() == 0) return;
@@ -329,8 +331,10 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
                              const pramaan_warm_start* warm)
     : opt_(opt) {
     validate_options(opt);
-    if (opt.algorithm != PRAMAAN_ALGO_ADAPTIVE)
-        throw InvalidArgument("batched solves use the adaptive algorithm (PRAMAAN_ALGO_ADAPTIVE)");
+    if (opt.algorithm != PRAMAAN_ALGO_ADAPTIVE && opt.algorithm != PRAMAAN_ALGO_HALPERN)
+        throw InvalidArgument("batched solves use the adaptive or the Halpern algorithm "
+                              "(PRAMAAN_ALGO_ADAPTIVE, PRAMAAN_ALGO_HALPERN)");
+    halpern_ = opt.algorithm == PRAMAAN_ALGO_HALPERN;
     if (count < 0) throw InvalidArgument("batch: count must be >= 0");
     dev_ = opt.device;
     count_ = count;
@@ -465,6 +469,17 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     chunk_out_.alloc(size_t(std::max(rseg_.chunks, cseg_.chunks)) * 4 + 4);
     lp_out_.alloc(size_t(K_) * kOutWidth);
     action_.alloc(K_); inv_.alloc(K_); keep_.alloc(K_); dscale_.alloc(K_); pscale_.alloc(K_); lp_f_.alloc(K_);
+    if (halpern_) {
+        restart_iter_.alloc(K_);
+        iter_base_.alloc(1);
+        PB_CUDA_CHECK(cudaMallocHost(&h_restart_iter_, sizeof(int) * K_));
+        for (int q = 0; q < K_; ++q) h_restart_iter_[q] = 0;
+        PB_CUDA_CHECK(cudaMemcpyAsync(restart_iter_.get(), h_restart_iter_, sizeof(int) * K_, cudaMemcpyHostToDevice, st_));
+        for (int b = 0; b < 2; ++b) {
+            fpr_c_[b].alloc(n_);
+            fpr_r_[b].alloc(m_ > 0 ? m_ : 1);
+        }
+    }
     ones_.alloc(2);
     fill_kernel<<<1, 32, 0, st_>>>(ones_.get(), 2, 1.0f);
     PB_CUDA_CHECK(cudaGetLastError());
@@ -524,6 +539,7 @@ AdaptiveBatch::~AdaptiveBatch() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (graph_) cudaGraphDestroy(graph_);
     if (h_action_) cudaFreeHost(h_action_);
+    if (h_restart_iter_) cudaFreeHost(h_restart_iter_);
     if (h_inv_) cudaFreeHost(h_inv_);
     if (h_dscale_) cudaFreeHost(h_dscale_);
     if (h_pscale_) cudaFreeHost(h_pscale_);
@@ -683,7 +699,26 @@ void AdaptiveBatch::apply_steps() {
     PB_CUDA_CHECK(cudaGetLastError());
 }
 
-void AdaptiveBatch::iterate_once() {
+void AdaptiveBatch::iterate_once(int j, int k) {
+    if (halpern_) {
+        // primal first (A^T y), then the dual with the extrapolated primal (A x̄)
+        double* fc = j == 0 ? fpr_c_[0].get() : (j == k - 1 ? fpr_c_[1].get() : nullptr);
+        double* fr = j == 0 ? fpr_r_[0].get() : (j == k - 1 ? fpr_r_[1].get() : nullptr);
+        // the anchor is the restart point, which the fold made the master: 0 in correction space
+        const float* ax = nullptr;
+        const float* ay = nullptr;
+        EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(), ax, lp_col_.get(),
+                            restart_iter_.get(), iter_base_.get(), j, fc};
+        SpmvLauncher<EpiPrimalHalpern, float, float, false>::launch(AT_.view(false), y_.get(), ep, status_.get(), st_,
+                                                                   dev_);
+        if (m_ > 0) {
+            EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), ay, lp_row_.get(),
+                              restart_iter_.get(), iter_base_.get(), j, fr};
+            SpmvLauncher<EpiDualHalpern, float, float, false>::launch(A_.view(false), xbar_.get(), ed, status_.get(),
+                                                                     st_, dev_);
+        }
+        return;
+    }
     if (m_ > 0) {
         EpiDualAdapt epi{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), ysum_.get(), ones_.get()};
         SpmvLauncher<EpiDualAdapt, float, float, false>::launch(A_.view(false), xbar_.get(), epi, status_.get(), st_, dev_);
@@ -692,29 +727,38 @@ void AdaptiveBatch::iterate_once() {
     SpmvLauncher<EpiPrimalAdapt, float, float, false>::launch(AT_.view(false), y_.get(), epi, status_.get(), st_, dev_);
 }
 
-void AdaptiveBatch::iterate(int k) {
+void AdaptiveBatch::iterate(int k, int iter) {
     if (k <= 0) return;
+    if (halpern_) {
+        set_int_kernel<<<1, 1, 0, st_>>>(iter_base_.get(), iter);
+        PB_CUDA_CHECK(cudaGetLastError());
+    }
     if (!opt_.use_graph || k > 4096) {
-        for (int i = 0; i < k; ++i) iterate_once();
-        return;
-    }
-    if (graph_iters_ != k) {
-        if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
-        if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
-        PB_CUDA_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-        try {
-            for (int i = 0; i < k; ++i) iterate_once();
-        } catch (...) {
-            cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(st_, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
+        for (int i = 0; i < k; ++i) iterate_once(i, k);
+    } else {
+        if (graph_iters_ != k) {
+            if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
+            if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+            PB_CUDA_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+            try {
+                for (int i = 0; i < k; ++i) iterate_once(i, k);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(st_, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            PB_CUDA_CHECK(cudaStreamEndCapture(st_, &graph_));
+            PB_CUDA_CHECK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+            graph_iters_ = k;
         }
-        PB_CUDA_CHECK(cudaStreamEndCapture(st_, &graph_));
-        PB_CUDA_CHECK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
-        graph_iters_ = k;
+        PB_CUDA_CHECK(cudaGraphLaunch(graph_exec_, st_));
     }
-    PB_CUDA_CHECK(cudaGraphLaunch(graph_exec_, st_));
+    if (halpern_ && k == 1) {
+        // the only iteration is both the first and the last one
+        PB_CUDA_CHECK(cudaMemcpyAsync(fpr_c_[1].get(), fpr_c_[0].get(), size_t(n_) * 8, cudaMemcpyDeviceToDevice, st_));
+        if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(fpr_r_[1].get(), fpr_r_[0].get(), size_t(m_) * 8, cudaMemcpyDeviceToDevice, st_));
+    }
 }
 
 void AdaptiveBatch::materialize_average() {
@@ -725,12 +769,13 @@ void AdaptiveBatch::materialize_average() {
     PB_CUDA_CHECK(cudaGetLastError());
 }
 
-void AdaptiveBatch::kkt(std::vector<KktSums>& cur, std::vector<KktSums>& avg) {
-    materialize_average();
+void AdaptiveBatch::kkt(std::vector<KktSums>& cur, std::vector<KktSums>& avg, bool with_average) {
+    if (with_average) materialize_average();
     const float* xs[2] = {x_.get(), xa_.get()};
     const float* ys[2] = {y_.get(), ya_.get()};
-    if (m_ == 0) PB_CUDA_CHECK(cudaMemsetAsync(lp_out_.get(), 0, lp_out_.bytes(), st_));
-    for (int k = 0; k < 2; ++k) {
+    const int candidates = with_average ? 2 : 1;
+    if (m_ == 0 || !with_average) PB_CUDA_CHECK(cudaMemsetAsync(lp_out_.get(), 0, lp_out_.bytes(), st_));
+    for (int k = 0; k < candidates; ++k) {
         if (m_ > 0) {
             EpiRowKktOut er{rlo64_.get(), rhi64_.get(), actm64_.get(), ym64_.get(), ys[k], rcon_.get()};
             launch_any<EpiRowKktOut, double, float>(A_, xs[k], er, status_.get(), st_, dev_);
@@ -815,8 +860,15 @@ void AdaptiveBatch::solve(const pramaan_lp* lps, pramaan_solve_result* results) 
             PB_CUDA_CHECK(cudaMemsetAsync(xl_.get(), 0, xl_.bytes(), st_));
             if (m_) PB_CUDA_CHECK(cudaMemsetAsync(yl_.get(), 0, yl_.bytes(), st_));
         }
+        if (halpern_) {
+            solve_halpern();
+            const double ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            finish(lps, results, ms);
+            return;
+        }
         std::vector<KktSums> cur, avg;
-        kkt(cur, avg);
+        kkt(cur, avg, true);
         for (int q = 0; q < K_; ++q) {
             Lp& s = lp_[q];
             s.kkt_restart = weighted(cur[q].pr2, cur[q].dr2, cur[q].pobj - cur[q].dobj, s.omega);
@@ -834,10 +886,10 @@ void AdaptiveBatch::solve(const pramaan_lp* lps, pramaan_solve_result* results) 
         };
         while (any_active() && iter < max_it) {
             const int chunk = std::min(cf, max_it - iter);
-            iterate(chunk);
+            iterate(chunk, iter);
             iter += chunk;
             for (Lp& s : lp_) if (s.active) s.avg_count += chunk;
-            kkt(cur, avg);
+            kkt(cur, avg, true);
             bool any_action = false, any_restart = false, steps_changed = false;
             for (int q = 0; q < K_; ++q) {
                 Lp& s = lp_[q];
@@ -938,6 +990,144 @@ void AdaptiveBatch::solve(const pramaan_lp* lps, pramaan_solve_result* results) 
     }
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     finish(lps, results, ms);
+}
+
+// Restarted Halpern PDHG (PRAMAAN_ALGO_HALPERN): the iteration of
+// EpiPrimalHalpern / EpiDualHalpern, restarts of each LP at its current
+// iterate when its fixed-point residual r = ||z - T(z)|| (step-weighted)
+// falls to 0.2 of its value at the last restart, or to 0.8 of it while
+// growing, or after 0.36 of all iterations since that restart; termination
+// on the relative KKT error of the current iterate.
+void AdaptiveBatch::solve_halpern() {
+    constexpr double kSufficient = 0.2, kNecessary = 0.8, kArtificial = 0.36;
+    constexpr int kFrozen = INT_MIN / 4;   // restart iteration of a frozen LP: weight 1
+    const int cf = opt_.check_frequency;
+    const int max_it = opt_.max_iterations;
+    const double tol = opt_.tolerance;
+    const bool refine = opt_.refine != 0;
+    auto converged = [&](const Lp& s, const KktSums& o, double& rp, double& rd, double& rg) {
+        rp = std::sqrt(o.pr2) / (1.0 + s.b_norm);
+        rd = std::sqrt(o.dr2) / (1.0 + s.c_norm);
+        rg = std::fabs(o.pobj - o.dobj) / (1.0 + std::fabs(o.pobj) + std::fabs(o.dobj));
+        return rp <= tol && rd <= tol && rg <= tol;
+    };
+    std::vector<KktSums> cur, avg;
+    kkt(cur, avg, false);
+    for (int q = 0; q < K_; ++q) {
+        Lp& s = lp_[q];
+        s.need_fpr0 = true;
+        s.fpr_prev = std::numeric_limits<double>::infinity();
+        s.last_restart = 0;
+        h_restart_iter_[q] = 0;
+        if (converged(s, cur[q], s.rel_p, s.rel_d, s.rel_gap)) {
+            s.status = PRAMAAN_STATUS_OPTIMAL;
+            s.active = false;
+            h_restart_iter_[q] = kFrozen;
+        }
+    }
+    PB_CUDA_CHECK(cudaMemcpyAsync(restart_iter_.get(), h_restart_iter_, sizeof(int) * K_, cudaMemcpyHostToDevice, st_));
+    apply_steps();
+    int iter = 0;
+    auto any_active = [&] {
+        for (const Lp& s : lp_) if (s.active) return true;
+        return false;
+    };
+    while (any_active() && iter < max_it) {
+        const int chunk = std::min(cf, max_it - iter);
+        iterate(chunk, iter);
+        iter += chunk;
+        kkt(cur, avg, false);
+        // fixed-point residual of the interval's first and last iteration (slots 8-11)
+        reduce(cseg_, fpr_c_[0].get(), 1, false, 8);
+        reduce(cseg_, fpr_c_[1].get(), 1, false, 10);
+        if (m_) {
+            reduce(rseg_, fpr_r_[0].get(), 1, false, 9);
+            reduce(rseg_, fpr_r_[1].get(), 1, false, 11);
+        }
+        fetch_out();
+        bool any_restart = false, steps_changed = false, restart_changed = false;
+        for (int q = 0; q < K_; ++q) {
+            Lp& s = lp_[q];
+            h_action_[q] = kActNone;
+            if (!s.active) continue;
+            ++s.checks;
+            const double* o = h_out_ + size_t(q) * kOutWidth;
+            const double r_first = std::sqrt(o[8] + (m_ ? o[9] : 0.0));
+            const double r_last = std::sqrt(o[10] + (m_ ? o[11] : 0.0));
+            if (s.need_fpr0) {
+                s.fpr0 = r_first;
+                s.need_fpr0 = false;
+            }
+            double rp, rd, rg;
+            const bool done = !cur[q].bad && converged(s, cur[q], rp, rd, rg);
+            if (cur[q].bad || !std::isfinite(r_last)) {
+                s.status = PRAMAAN_STATUS_NUMERICAL_FAILURE;
+            } else if (done) {
+                s.status = PRAMAAN_STATUS_OPTIMAL;
+            }
+            if (cur[q].bad || !std::isfinite(r_last) || done) {
+                if (done) { s.rel_p = rp; s.rel_d = rd; s.rel_gap = rg; }
+                s.iterations = iter;
+                s.active = false;
+                h_restart_iter_[q] = kFrozen;
+                steps_changed = restart_changed = true;
+                continue;
+            }
+            s.rel_p = rp; s.rel_d = rd; s.rel_gap = rg;
+            const bool restart = r_last <= kSufficient * s.fpr0 ||
+                                 (r_last <= kNecessary * s.fpr0 && r_last > s.fpr_prev) ||
+                                 (iter - s.last_restart) >= kArtificial * iter;
+            s.fpr_prev = r_last;
+            if (!restart) continue;
+            h_action_[q] = kActRestartCurrent;
+            any_restart = restart_changed = true;
+            s.fpr_prev = std::numeric_limits<double>::infinity();
+            s.need_fpr0 = true;
+            s.last_restart = iter;
+            h_restart_iter_[q] = iter;
+            ++s.restarts;
+        }
+        if (any_restart) {
+            push_actions();
+            // movement since the previous restart point, in the scaled norms
+            dist_contrib_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(x_.get(), refine ? nullptr : xl_.get(),
+                                                                   cscale_.get(), n_, ccon_.get());
+            PB_CUDA_CHECK(cudaGetLastError());
+            reduce(cseg_, ccon_.get(), 1, false, 0);
+            if (m_) {
+                dist_contrib_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(y_.get(), refine ? nullptr : yl_.get(),
+                                                                       rscale_.get(), m_, rcon_.get());
+                PB_CUDA_CHECK(cudaGetLastError());
+                reduce(rseg_, rcon_.get(), 1, false, 1);
+            }
+            fetch_out();
+            for (int q = 0; q < K_; ++q) {
+                if (h_action_[q] != kActRestartCurrent) continue;
+                Lp& s = lp_[q];
+                const double dx = std::sqrt(h_out_[size_t(q) * kOutWidth + 0]);
+                const double dy = m_ ? std::sqrt(h_out_[size_t(q) * kOutWidth + 1]) : 0.0;
+                if (dx > 1e-10 && dy > 1e-10) {
+                    const double w = std::exp(0.5 * std::log(dy / dx) + 0.5 * std::log(s.omega));
+                    if (std::isfinite(w) && w > 0.0) { s.omega = w; steps_changed = true; }
+                }
+            }
+            if (refine) {
+                fold(false);   // the restart point becomes the master: the anchor is 0 again
+            } else {
+                record_lp_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(lp_col_.get(), action_.get(), n_, x_.get(), xl_.get());
+                if (m_) record_lp_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(lp_row_.get(), action_.get(), m_, y_.get(), yl_.get());
+                PB_CUDA_CHECK(cudaGetLastError());
+            }
+        }
+        if (restart_changed)
+            PB_CUDA_CHECK(cudaMemcpyAsync(restart_iter_.get(), h_restart_iter_, sizeof(int) * K_, cudaMemcpyHostToDevice, st_));
+        if (steps_changed) apply_steps();
+        long long live = 0;
+        for (const Lp& s : lp_) if (s.active) live += s.nnz;
+        if (live > 0 && 2 * live < (long long)nnz_ && (long long)nnz_ - live >= 65536) compact();
+    }
+    for (Lp& s : lp_)
+        if (s.status == PRAMAAN_STATUS_ITERATION_LIMIT) s.iterations = max_it;
 }
 
 void AdaptiveBatch::scatter_answers(const int* keep) {

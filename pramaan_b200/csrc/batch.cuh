@@ -67,6 +67,10 @@ private:
         int status = PRAMAAN_STATUS_ITERATION_LIMIT;
         int iterations = 0, restarts = 0, checks = 0;
         bool active = true;
+        // Halpern mode: fixed-point residual at the last restart point and at
+        // the previous check (the restart tests compare against them)
+        double fpr0 = 0, fpr_prev = 0;
+        bool need_fpr0 = true;
         double rel_p = 0, rel_d = 0, rel_gap = 0;
     };
     struct Segments {                  // chunk table of one side (rows or columns)
@@ -83,9 +87,13 @@ private:
     void preconditioned_steps();
     void estimate_step_sizes();
     void apply_steps();
-    void iterate(int k);
-    void iterate_once();
-    void kkt(std::vector<KktSums>& cur, std::vector<KktSums>& avg);
+    // k iterations starting at global iteration `iter`
+    void iterate(int k, int iter);
+    // iteration j of an interval of k (Halpern mode writes the fixed-point
+    // residual on the first and the last one)
+    void iterate_once(int j, int k);
+    void kkt(std::vector<KktSums>& cur, std::vector<KktSums>& avg, bool with_average);
+    void solve_halpern();
     void materialize_average();
     void push_actions();
     void fold(bool first);
@@ -128,6 +136,10 @@ private:
     DevBuf<double> xsum_, ysum_, xm64_, ym64_, actm64_, rcm64_;
     DevBuf<double> rcon_, ccon_, chunk_out_, lp_out_;
     DevBuf<int> action_;
+    bool halpern_ = false;             // PRAMAAN_ALGO_HALPERN
+    DevBuf<int> restart_iter_, iter_base_;   // per LP: iteration of the last restart; the interval's first iteration
+    int* h_restart_iter_ = nullptr;
+    DevBuf<double> fpr_c_[2], fpr_r_[2];     // fixed-point residual terms, first / last iteration of an interval
     DevBuf<double> xw_, yw_;           // warm start (original layout), empty when cold
     DevBuf<double> inv_;
     DevBuf<float> dscale_, pscale_, lp_f_;

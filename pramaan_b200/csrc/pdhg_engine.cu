@@ -108,16 +108,19 @@ void validate_options(const pramaan_pdhg_options& opt) {
     if (opt.check_frequency < 1) throw InvalidArgument("pdhg options: check_frequency must be >= 1");
     if (opt.max_iterations < 0) throw InvalidArgument("pdhg options: max_iterations must be >= 0");
     if (!(opt.tolerance >= 0.0)) throw InvalidArgument("pdhg options: tolerance must be >= 0");
-    if (opt.algorithm != PRAMAAN_ALGO_REFERENCE && opt.algorithm != PRAMAAN_ALGO_ADAPTIVE)
+    if (opt.algorithm != PRAMAAN_ALGO_REFERENCE && opt.algorithm != PRAMAAN_ALGO_ADAPTIVE &&
+        opt.algorithm != PRAMAAN_ALGO_HALPERN)
         throw InvalidArgument("pdhg options: unknown algorithm");
     if (opt.termination != PRAMAAN_TERM_REFERENCE && opt.termination != PRAMAAN_TERM_RELATIVE_KKT)
         throw InvalidArgument("pdhg options: unknown termination criterion");
     if (opt.algorithm == PRAMAAN_ALGO_REFERENCE && opt.termination != PRAMAAN_TERM_REFERENCE)
         throw InvalidArgument("pdhg options: the reference algorithm uses the reference criterion");
-    if (opt.algorithm == PRAMAAN_ALGO_ADAPTIVE && opt.termination != PRAMAAN_TERM_RELATIVE_KKT)
-        throw InvalidArgument("pdhg options: the adaptive algorithm terminates on the relative KKT error "
-                              "(PRAMAAN_TERM_RELATIVE_KKT)");
+    if (opt.algorithm != PRAMAAN_ALGO_REFERENCE && opt.termination != PRAMAAN_TERM_RELATIVE_KKT)
+        throw InvalidArgument("pdhg options: the adaptive and Halpern algorithms terminate on the relative KKT "
+                              "error (PRAMAAN_TERM_RELATIVE_KKT)");
     if (opt.refine != 0 && opt.refine != 1) throw InvalidArgument("pdhg options: refine must be 0 or 1");
+    if (opt.algorithm == PRAMAAN_ALGO_HALPERN && opt.refine != 1)
+        throw InvalidArgument("pdhg options: the Halpern algorithm runs on FP64 master iterates (refine = 1)");
 }
 
 PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : opt_(opt) {

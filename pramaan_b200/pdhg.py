@@ -18,7 +18,7 @@ from . import _lib as L
 kInfinity = 1.0e30   # include/pramaan/ir.hpp:47
 
 # PdhgOptions.algorithm / .termination values (include/pramaan_b200.h)
-ALGO_REFERENCE, ALGO_ADAPTIVE = 0, 1
+ALGO_REFERENCE, ALGO_ADAPTIVE, ALGO_HALPERN = 0, 1, 2
 TERM_REFERENCE, TERM_RELATIVE_KKT = 0, 1
 
 
@@ -122,7 +122,7 @@ class PdhgOptions:
     tolerance: float = 1e-6
     max_iterations: int = 100000
     check_frequency: int = 100
-    algorithm: int = 0          # 0: the reference iteration, 1: adaptive
+    algorithm: int = 0          # 0: the reference iteration, 1: adaptive (PDLP-style), 2: Halpern
     termination: int | None = None  # default: reference criterion / relative KKT (adaptive)
     device: int = 0
     use_graph: bool = True
@@ -137,7 +137,7 @@ class PdhgOptions:
         o.check_frequency = int(self.check_frequency)
         o.algorithm = int(self.algorithm)
         if self.termination is None:
-            o.termination = TERM_RELATIVE_KKT if int(self.algorithm) == ALGO_ADAPTIVE else TERM_REFERENCE
+            o.termination = TERM_REFERENCE if int(self.algorithm) == ALGO_REFERENCE else TERM_RELATIVE_KKT
         else:
             o.termination = int(self.termination)
         o.device = int(self.device)
@@ -210,16 +210,16 @@ class PdhgSolver:
     def solve_batch(self, models: list[ModelIR]) -> list[SolveResult]:
         """Solves many LPs in one packed launch sequence (pramaan_pdhg_solve_batch).
 
-        Uses the adaptive algorithm with relative-KKT termination whatever
-        ``options.algorithm`` says; each LP keeps its own step size, weight,
-        restarts and termination.
+        Uses the Halpern algorithm when ``options.algorithm`` is ALGO_HALPERN and
+        the adaptive algorithm otherwise, with relative-KKT termination; each LP
+        keeps its own step size, weight, restarts and termination.
         """
         return solve_batch(models, self.options)
 
 
 def solve_batch(models: list[ModelIR], options: PdhgOptions | None = None,
                 warm: list | None = None) -> list[SolveResult]:
-    """Batched adaptive PDHG over ``models`` (see ``PdhgSolver.solve_batch``).
+    """Batched PDHG over ``models`` (see ``PdhgSolver.solve_batch``).
 
     ``warm`` (optional) gives each LP a starting point: an object with
     attributes ``x``, ``y`` (arrays or None) and ``primal_weight`` (a float,
@@ -227,7 +227,7 @@ def solve_batch(models: list[ModelIR], options: PdhgOptions | None = None,
     (pramaan_pdhg_solve_batch_warm)."""
     opts = options or PdhgOptions()
     o = opts.c_struct()
-    o.algorithm = ALGO_ADAPTIVE
+    o.algorithm = ALGO_HALPERN if int(opts.algorithm) == ALGO_HALPERN else ALGO_ADAPTIVE
     o.termination = TERM_RELATIVE_KKT
     k = len(models)
     lps = (L.CLp * max(k, 1))()

@@ -1,0 +1,84 @@
+"""GPU tests of the restarted Halpern PDHG mode (PRAMAAN_ALGO_HALPERN).
+
+The checker is the oracle's FP64 restatement oracle/adaptive.py
+(solve_halpern).  The device runs FP32 corrections around FP64 master
+iterates, so trajectories are not bit-identical; what is compared: the FP64
+relative KKT of the answer (oracle.rel_kkt) meets the tolerance, the
+objective equals the restatement's within the tolerance's reach, the
+iteration counts agree within a factor of 2, and the mode needs fewer
+iterations than the adaptive (PDLP-style) mode on the same LPs.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from lp_cases import KNOWN
+from oracle import adaptive as oad
+from pramaan_b200 import PdhgOptions, PdhgSolver, SolveStatus, solve_batch
+from pramaan_b200.generators import ill_conditioned_lp, random_sparse_lp, rolling_horizon_batch, rolling_horizon_lp
+from pramaan_b200.pdhg import ALGO_ADAPTIVE, ALGO_HALPERN
+
+pytestmark = pytest.mark.gpu
+
+
+def opts(tol, algo=ALGO_HALPERN, it=400000, refine=True):
+    return PdhgOptions(tolerance=tol, max_iterations=it, check_frequency=64, algorithm=algo, refine=refine)
+
+
+def lps():
+    return {"rh24x5": rolling_horizon_lp(24, 5, seed=1), "rand300": random_sparse_lp(300, 900, 4, seed=0),
+            "ill300": ill_conditioned_lp(300, 800, 4, seed=0, scale_exp=2), "wyndor": KNOWN["wyndor"][0]}
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-8])
+def test_single_solves_match_the_restatement(tol):
+    for name, md in lps().items():
+        r = PdhgSolver(opts(tol)).solve(md)
+        assert r.status == SolveStatus.kOptimal, (name, r.iterations)
+        k = oracle.rel_kkt(md, r.x, r.y)
+        assert max(k["primal"], k["dual"], k["gap"]) <= tol * 1.0001, (name, k)
+        ref = oad.solve_halpern(md, tol=tol, max_iterations=400000)
+        assert ref["status"] == "optimal"
+        scale = 1 + abs(ref["kkt"]["pobj"])
+        assert abs(k["pobj"] - ref["kkt"]["pobj"]) <= 20 * tol * scale, name
+        assert 0.5 * ref["iterations"] <= r.iterations <= 2.0 * ref["iterations"] + 128, (name, r.iterations,
+                                                                                          ref["iterations"])
+
+
+def test_halpern_requires_fp64_master_iterates():
+    with pytest.raises(ValueError, match="refine"):
+        PdhgSolver(opts(1e-6, refine=False)).solve(random_sparse_lp(30, 90, 3, seed=1))
+
+
+def test_batch_matches_single_solves_and_beats_the_adaptive_mode():
+    models = rolling_horizon_batch(12, seed=3, T_range=(24, 60), P_range=(5, 12))
+    hal = solve_batch(models, opts(1e-6))
+    ada = solve_batch(models, opts(1e-6, ALGO_ADAPTIVE))
+    for md, r in zip(models, hal):
+        assert r.status == SolveStatus.kOptimal
+        k = oracle.rel_kkt(md, r.x, r.y)
+        assert max(k["primal"], k["dual"], k["gap"]) <= 1e-6 * 1.0001
+        alone = PdhgSolver(opts(1e-6)).solve(md)
+        assert r.objective_value == pytest.approx(alone.objective_value, rel=1e-4, abs=1e-4)
+    assert sum(r.iterations for r in hal) < 0.8 * sum(r.iterations for r in ada)
+
+
+def test_batch_is_deterministic_and_handles_early_answers():
+    from pramaan_b200.pdhg import ModelIR
+    models = rolling_horizon_batch(6, seed=4, T_range=(24, 40), P_range=(5, 8))
+    empty = ModelIR([], [0, 0], [], [], [1.0], [2.0], [], [], 0, 4.5)
+    a = solve_batch(models + [empty, KNOWN["wyndor"][0]], opts(1e-7))
+    b = solve_batch(models + [empty, KNOWN["wyndor"][0]], opts(1e-7))
+    for ra, rb in zip(a, b):
+        assert ra.iterations == rb.iterations and np.array_equal(ra.x, rb.x)
+    assert a[-2].status == SolveStatus.kOptimal and a[-2].objective_value == 4.5
+    assert a[-1].objective_value == pytest.approx(36.0, rel=1e-6)
+
+
+def test_warm_start_from_the_solution_stops_early():
+    from pramaan_b200.gnn import training_targets
+    models = rolling_horizon_batch(4, seed=5, T_range=(24, 30), P_range=(5, 6))
+    cold = solve_batch(models, opts(1e-6))
+    warm = solve_batch(models, opts(1e-6), warm=training_targets(cold))
+    for c, w in zip(cold, warm):
+        assert w.status == SolveStatus.kOptimal and w.iterations <= 64 < c.iterations
