@@ -254,10 +254,10 @@ def rolling_horizon_section(args, device):
     LPs one by one (a sample of them)."""
     from pramaan_b200 import PdhgOptions, PdhgSolver, SolveStatus, solve_batch
     from pramaan_b200.generators import rolling_horizon_batch
-    from pramaan_b200.pdhg import ALGO_ADAPTIVE
+    from pramaan_b200.pdhg import ALGO_HALPERN
 
     tol = 1e-6
-    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_ADAPTIVE,
+    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)
     models = rolling_horizon_batch(args.rh_count, seed=args.seed)
     solve_batch(models[:2], o)                       # warm-up (module load, occupancy queries)
@@ -276,7 +276,7 @@ def rolling_horizon_section(args, device):
     batched = len(models) / tb
     plain = len(idx) / sum(plain_t)
     return {"workload": f"rolling_horizon_batch {len(models)} LPs (T~U{{24..336}}, P~U{{5..50}}), "
-                        f"rel KKT {tol:g}, seed {args.seed}",
+                        f"rel KKT {tol:g}, seed {args.seed}; restarted Halpern PDHG, batched and one by one",
             "rows": sum(m.numRows() for m in models), "cols": sum(m.numVars() for m in models),
             "nnz": sum(m.nnz() for m in models),
             "batched_lps_per_s": batched, "batched_s": tb, "batched_iterations_median": float(np.median(its)),
@@ -295,7 +295,7 @@ def learned_stream_section(args, device):
     shifted solution alone."""
     from pramaan_b200 import PdhgOptions, SolveStatus, solve_batch
     from pramaan_b200.gnn import WarmStartNet, warm_solve_batch
-    from pramaan_b200.pdhg import ALGO_ADAPTIVE
+    from pramaan_b200.pdhg import ALGO_HALPERN
     from pramaan_b200.train_warm_start import DEFAULT_OUT, stream_windows
 
     if not DEFAULT_OUT.exists():
@@ -304,7 +304,7 @@ def learned_stream_section(args, device):
     net = WarmStartNet(device=device, seed=0)
     net.load(DEFAULT_OUT)
     tol = 1e-6
-    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_ADAPTIVE,
+    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)
     S, W = args.stream_count, args.stream_windows
     ms, _ = stream_windows(range(700000 + args.seed, 700000 + args.seed + S), W, tuple(rec["T"]), tuple(rec["P"]))

@@ -6,7 +6,7 @@ Usage:
 
 Generates S streams of W consecutive windows (rolling_horizon_stream: AR(1)
 demand, the window shifting by one period), labels every window with the
-batched adaptive PDHG at 1e-6 relative KKT, builds each window's hint (the
+batched restarted Halpern PDHG at 1e-6 relative KKT, builds each window's hint (the
 previous window's solution shifted by one period; none for a stream's first
 window) and fits the network with Adam on mini-batches of 16 hinted windows.
 The labels are the PDHG's own solutions, so the network learns nothing the
@@ -29,7 +29,7 @@ if __package__ in (None, ""):
 from pramaan_b200 import PdhgOptions, SolveStatus, solve_batch  # noqa: E402
 from pramaan_b200.generators import rolling_horizon_shift, rolling_horizon_stream  # noqa: E402
 from pramaan_b200.gnn import WarmStart, WarmStartNet, training_targets  # noqa: E402
-from pramaan_b200.pdhg import ALGO_ADAPTIVE  # noqa: E402
+from pramaan_b200.pdhg import ALGO_HALPERN  # noqa: E402
 
 DEFAULT_OUT = Path(__file__).resolve().parent / "weights" / "warm_start_rolling_horizon.npz"
 
@@ -71,7 +71,7 @@ def main(argv=None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", type=Path, default=DEFAULT_OUT)
     a = ap.parse_args(argv)
-    o = PdhgOptions(tolerance=1e-6, max_iterations=300000, check_frequency=64, algorithm=ALGO_ADAPTIVE,
+    o = PdhgOptions(tolerance=1e-6, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=a.device)
     t0 = time.time()
     models, first = stream_windows(range(a.seed0, a.seed0 + a.streams), a.windows, tuple(a.T), tuple(a.P))
