@@ -353,6 +353,33 @@ def learned_stream_section(args, device):
     return out
 
 
+def small_lp_section(args, device):
+    """The plain-PDHG LP (m = 1000, n = 3000, 4 non-zeros per column, N(0,1)
+    values, feasible by construction): time to 1e-4 with the reference
+    algorithm and criterion, and with the Halpern mode to 1e-4 / 1e-8 relative
+    KKT (FP64 certificate of each answer)."""
+    from pramaan_b200 import PdhgOptions, PdhgSolver
+    from pramaan_b200.certificate import certify
+    from pramaan_b200.generators import random_sparse_lp
+    from pramaan_b200.pdhg import ALGO_HALPERN
+
+    md = random_sparse_lp(1000, 3000, 4, seed=args.seed)
+    out = {"workload": f"random_sparse_lp 1000 x 3000, 4 nnz/col, seed {args.seed}"}
+    PdhgSolver(PdhgOptions(tolerance=1e-4, device=device)).solve(md)          # warm-up
+    for name, o in (("reference_1e-4", PdhgOptions(tolerance=1e-4, device=device)),
+                    ("halpern_1e-4", PdhgOptions(tolerance=1e-4, algorithm=ALGO_HALPERN, check_frequency=64,
+                                                 device=device)),
+                    ("halpern_1e-8", PdhgOptions(tolerance=1e-8, algorithm=ALGO_HALPERN, check_frequency=64,
+                                                 max_iterations=400000, device=device))):
+        t0 = time.perf_counter()
+        r = PdhgSolver(o).solve(md)
+        dt = time.perf_counter() - t0
+        c = certify(md, r.x, r.y, device)
+        out[name] = {"status": r.status.name, "iterations": r.iterations, "seconds": dt,
+                     "rel_kkt": c.kkt, "objective": r.objective_value}
+    return out
+
+
 def _hints_for(batch, prev):
     """Each stream's previous window solution shifted onto its current window."""
     from pramaan_b200 import SolveStatus
@@ -477,6 +504,7 @@ def run_gpu_arm(args):
                        "call_s_median": statistics.median(times)}
 
     if not args.no_rolling:
+        line["small_lp"] = small_lp_section(args, local)
         line["rolling_horizon"] = rolling_horizon_section(args, local)
         line["learned_stream"] = learned_stream_section(args, local)
     if rank == 0 and not args.no_cpu_baseline:

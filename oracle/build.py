@@ -102,6 +102,15 @@ def build_reference(force: bool = False) -> dict[str, Path]:
     if force or not _newer(facade_obj, facade):
         jobs.append([*cxx, *inc, "-I", str(REPO / "include"), "-c", str(facade), "-o",
                      str(facade_obj)])
+    # the GPU Backend of the facade and its check program (ours, against the reference's headers)
+    backend = REPO / "pramaan_b200" / "csrc" / "facade" / "cuda_backend.cpp"
+    backend_obj = obj_dir / "facade_cuda_backend.o"
+    if force or not _newer(backend_obj, backend, backend.with_suffix(".hpp")):
+        jobs.append([*cxx, *inc, "-I", str(REPO / "include"), "-c", str(backend), "-o", str(backend_obj)])
+    bcheck = REPO / "tests" / "cpp" / "check_cuda_backend.cpp"
+    bcheck_obj = obj_dir / "check_cuda_backend.o"
+    if force or not _newer(bcheck_obj, bcheck, backend.with_suffix(".hpp")):
+        jobs.append([*cxx, *inc, "-I", str(backend.parent), "-c", str(bcheck), "-o", str(bcheck_obj)])
     # the reference's precision-ladder controller, compiled with its GPU rung enabled
     ladder_src = REF_SRC / "src" / "gpu" / "precision_ladder.cpp"
     ladder_obj = obj_dir / "precision_ladder_cuda.o"
@@ -144,6 +153,10 @@ def build_reference(force: bool = False) -> dict[str, Path]:
         _run(["g++", "-o", str(exe), str(obj), *extra, str(facade_obj), *core_objs,
               f"-L{lib_dir}", "-lpramaan_b200", f"-Wl,-rpath,$ORIGIN/../../pramaan_b200"])
         out[f"{t}__pramaan_b200"] = exe
+    exe = REF_OUT / "check_cuda_backend"
+    _run(["g++", "-o", str(exe), str(bcheck_obj), str(backend_obj), *core_objs,
+          f"-L{lib_dir}", "-lpramaan_b200", f"-Wl,-rpath,$ORIGIN/../../pramaan_b200"])
+    out["check_cuda_backend"] = exe
     # The reference's MPS fixtures, for the programs above (they open
     # tests/data/*.mps relative to their working directory).
     data = REF_OUT / "run" / "tests" / "data"

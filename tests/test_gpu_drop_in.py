@@ -37,3 +37,11 @@ def test_reference_program_on_reference_library(prog):
     rc, out = run(f"{prog}__reference")
     print(out[-3000:])
     assert "checks run" in out
+
+
+def test_cuda_backend_matches_the_cpu_backend():
+    """pramaan::gpu::make_cuda_backend() (the facade's Backend,
+    include/pramaan/gpu/backend.hpp:36-57) against the reference's CPU backend
+    on the same models (tests/cpp/check_cuda_backend.cpp)."""
+    rc, out = run("check_cuda_backend")
+    assert rc == 0 and "CUDA BACKEND CHECK PASSED" in out, out[-3000:]
