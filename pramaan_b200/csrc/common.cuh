@@ -105,6 +105,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
+// Programmatic dependent launch.  A kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may start while the
+// previous kernel of its stream is still running; grid_dep_wait() blocks
+// until that kernel has completed and its memory is visible, so everything
+// before it may only read data no kernel writes (tile records, constants).
+// grid_dep_launch() lets the next such kernel be scheduled early.  Both are
+// no-ops for kernels launched without the attribute.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // L2 eviction-priority policy for streamed (read-once) data.
 __device__ __forceinline__ uint64_t l2_policy_evict_first() {
     uint64_t pol;

@@ -26,6 +26,7 @@
 #include <atomic>
 #include <stdexcept>
 #include <cstddef>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -142,6 +143,24 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status);
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
 
+// Launches `k` with programmatic stream serialization, so that it may start
+// while the previous kernel of the stream finishes (the kernels wait with
+// grid_dep_wait() before touching anything that kernel may write).
+template <typename... KArgs, typename... Args>
+void launch_dependent(void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+}
+
 template <class Epi, typename AccT, typename XT, bool kLo>
 struct SpmvLauncher {
     using L = SpmvSmemLayout<kSpmvWarps, kSpmvStages, kLo, AccT>;
@@ -198,20 +217,15 @@ struct SpmvLauncher {
         if (A.num_tiles > 0) {
             const bool mapped = A.row_map != nullptr;
             const int grid = grid_for(A, dev);
-            if (mapped) {
-                auto k = kernel<true>();
-                k<<<grid, kSpmvWarps * 32, L::bytes, st>>>(A, x, epi, dev_status);
-            } else {
-                auto k = kernel<false>();
-                k<<<grid, kSpmvWarps * 32, L::bytes, st>>>(A, x, epi, dev_status);
-            }
-            PB_CUDA_CHECK(cudaGetLastError());
+            if (mapped)
+                launch_dependent(kernel<true>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
+            else
+                launch_dependent(kernel<false>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
         }
         const int fix = A.num_cross + A.num_empty;
         if (fix > 0) {
             const int grid = (fix + 255) / 256 < 2048 ? (fix + 255) / 256 : 2048;
-            spmv_fixup_kernel<Epi, AccT><<<grid, 256, 0, st>>>(A, epi);
-            PB_CUDA_CHECK(cudaGetLastError());
+            launch_dependent(&spmv_fixup_kernel<Epi, AccT>, grid, 256, 0, st, A, epi);
         }
     }
     // Kernels one launch() call issues.

@@ -173,6 +173,11 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
         const int pre = mine < STAGES ? mine : STAGES;
         for (int i = 0; i < pre; ++i) issue(i);
     }
+    // The tile records are never written while products run, so the first
+    // copies above may overlap the previous kernel; x, the epilogue's vectors
+    // and carry[] are touched only after it has completed.
+    grid_dep_launch();
+    grid_dep_wait();
 
     AccT* carry = reinterpret_cast<AccT*>(A.carry);
     bool failed = false;
@@ -319,6 +324,8 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
 template <class Epi, typename AccT>
 __global__ void __launch_bounds__(256)
     spmv_fixup_kernel(const CsrView A, const Epi epi) {
+    grid_dep_launch();
+    grid_dep_wait();
     typename Epi::State est;
     epi.init(est);
     const AccT* carry = reinterpret_cast<const AccT*>(A.carry);

@@ -45,6 +45,8 @@ int main() {
         m.var_lower = {0.0, 0.0};
         m.var_upper = {kInfinity, kInfinity};
         m.var_types = {VarType::kContinuous, VarType::kContinuous};
+        m.row_names = {"r0", "r1", "r2"};
+        m.var_names = {"x", "y"};
         compare("wyndor", m);
     }
     {   // min x + 2y + 3z, x + y + z = 5, x - y >= -1, 0 <= x,y,z <= 4
@@ -57,6 +59,8 @@ int main() {
         m.var_lower = {0.0, 0.0, 0.0};
         m.var_upper = {4.0, 4.0, 4.0};
         m.var_types = {VarType::kContinuous, VarType::kContinuous, VarType::kContinuous};
+        m.row_names = {"r0", "r1"};
+        m.var_names = {"x", "y", "z"};
         compare("equality", m);
     }
     try {
