@@ -101,7 +101,13 @@ typedef struct pramaan_pdhg_options {
                                  to about 1e-10 are reachable; 0: plain FP32
                                  iterates (resolution about 1e-6)               */
     double reserved_d;
-    int32_t reserved[6];
+    int32_t persistent;       /* Halpern mode: 1 runs each check interval as one
+                                 cooperative kernel (grid barriers between the
+                                 products); 0 (default) and -1 launch the two
+                                 products per iteration, captured in a CUDA graph
+                                 with dependent launches (faster on the measured
+                                 operands)                                      */
+    int32_t reserved[5];
 } pramaan_pdhg_options;
 
 /* Result, mirroring pramaan::SolveResult (include/pramaan/simplex.hpp:40-76).

@@ -93,6 +93,9 @@ private:
     // residual on the first and the last one)
     void iterate_once(int j, int k);
     void kkt(std::vector<KktSums>& cur, std::vector<KktSums>& avg, bool with_average);
+    // Halpern mode on small operands: one cooperative kernel per check interval
+    bool use_interval_kernel() const;
+    void launch_interval(int k);
     void solve_halpern();
     void materialize_average();
     void push_actions();
@@ -140,6 +143,7 @@ private:
     DevBuf<int> restart_iter_, iter_base_;   // per LP: iteration of the last restart; the interval's first iteration
     int* h_restart_iter_ = nullptr;
     DevBuf<double> fpr_c_[2], fpr_r_[2];     // fixed-point residual terms, first / last iteration of an interval
+    DevBuf<unsigned> gsync_;                 // grid barrier of the interval kernel {count, generation}
     DevBuf<double> xw_, yw_;           // warm start (original layout), empty when cold
     DevBuf<double> inv_;
     DevBuf<float> dscale_, pscale_, lp_f_;

@@ -119,6 +119,7 @@ void validate_options(const pramaan_pdhg_options& opt) {
         throw InvalidArgument("pdhg options: the adaptive and Halpern algorithms terminate on the relative KKT "
                               "error (PRAMAAN_TERM_RELATIVE_KKT)");
     if (opt.refine != 0 && opt.refine != 1) throw InvalidArgument("pdhg options: refine must be 0 or 1");
+    if (opt.persistent < -1 || opt.persistent > 1) throw InvalidArgument("pdhg options: persistent must be -1, 0 or 1");
     if (opt.algorithm == PRAMAAN_ALGO_HALPERN && opt.refine != 1)
         throw InvalidArgument("pdhg options: the Halpern algorithm runs on FP64 master iterates (refine = 1)");
 }

@@ -123,17 +123,25 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES>
-__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS)
-    spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
-                     int* __restrict__ dev_status) {
+// One product over the tiles of A, run by every warp of the grid (warp w of
+// block b takes tiles b*WARPS + w, + gridDim.x*WARPS, ...).  `used` counts the
+// tiles this warp's ring consumed in earlier products of the same kernel (0 and
+// `init_bars` for the first), so the ring's mbarrier phases carry over from one
+// product to the next.  `ready()` is called by every thread after the first
+// bulk copies are issued and before anything but the tile records is read or
+// written: a grid dependency wait, or a grid barrier in a multi-product
+// kernel; it returns false to abandon the product.  Returns false when a wait
+// gave up (the status word records it).
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, class Ready>
+__device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restrict__ x, const Epi& epi,
+                                           int* __restrict__ dev_status, unsigned char* smem, uint32_t& used,
+                                           bool init_bars, Ready&& ready) {
     using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT>;
     constexpr int IPT = kSpmvIpt;
     constexpr int TW = L::TW;
     constexpr int FW = L::FW;
     constexpr unsigned kMask = (IPT == 32) ? 0xffffffffu : ((1u << IPT) - 1u);
 
-    extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     unsigned char* ring = smem + size_t(warp) * L::warp_bytes;
@@ -152,15 +160,17 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
 
     uint64_t policy = 0;
     if (lane == 0) {
-        for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
-        fence_mbar_init();
+        if (init_bars) {
+            for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
+            fence_mbar_init();
+        }
         policy = l2_policy_evict_first();
     }
     __syncwarp();
 
     auto issue = [&](int i) {
         const int t = gw + i * stride;
-        const int s = i % STAGES;
+        const int s = int((used + uint32_t(i)) % STAGES);
         unsigned char* st = ring + size_t(s) * L::stage_bytes;
         const size_t off = size_t(t) * TW;
         mbar_arrive_expect_tx(&bar[s], L::tx_bytes);
@@ -174,18 +184,17 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
         for (int i = 0; i < pre; ++i) issue(i);
     }
     // The tile records are never written while products run, so the first
-    // copies above may overlap the previous kernel; x, the epilogue's vectors
-    // and carry[] are touched only after it has completed.
-    grid_dep_launch();
-    grid_dep_wait();
+    // copies above may overlap earlier work; x, the epilogue's vectors and
+    // carry[] are touched only once ready() has returned.
+    bool failed = !ready();
 
     AccT* carry = reinterpret_cast<AccT*>(A.carry);
-    bool failed = false;
     int i = 0;
-    for (; i < mine; ++i) {
+    for (; i < mine && !failed; ++i) {
         const int t = gw + i * stride;
-        const int s = i % STAGES;
-        const uint32_t parity = (i / STAGES) & 1;
+        const uint32_t u = used + uint32_t(i);
+        const int s = int(u % STAGES);
+        const uint32_t parity = (u / STAGES) & 1u;
         const bool ok = mbar_wait_bounded(&bar[s], parity);
         if (__any_sync(0xffffffffu, !ok)) {
             failed = true;
@@ -312,35 +321,61 @@ __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / 
             atomicOr(dev_status, kDevErrTimeout);
             // Let every bulk copy this warp issued land before it retires.
             const int hi = (i + STAGES) < mine ? (i + STAGES) : mine;
-            for (int j = i; j < hi; ++j) (void)mbar_wait_bounded(&bar[j % STAGES], (j / STAGES) & 1);
+            for (int j = i; j < hi; ++j) {
+                const uint32_t u = used + uint32_t(j);
+                (void)mbar_wait_bounded(&bar[u % STAGES], (u / STAGES) & 1u);
+            }
         }
         __syncwarp();
     }
+    used += uint32_t(mine);
     epi.finish(est, 0);
+    return !failed;
+}
+
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES>
+__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS)
+    spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
+                     int* __restrict__ dev_status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint32_t used = 0;
+    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES>(A, x, epi, dev_status, smem, used, true, [] {
+        grid_dep_launch();
+        grid_dep_wait();
+        return true;
+    });
 }
 
 // Finishes the rows that cross tiles (their pieces added in tile order) and
 // gives every empty row the value 0.
+// Thread `tid` of `nthreads` finishes its share of the crossing and empty
+// rows.  The pieces are read past L1 (they are written by other warps, and a
+// multi-product kernel reads them again after the next product).
 template <class Epi, typename AccT>
-__global__ void __launch_bounds__(256)
-    spmv_fixup_kernel(const CsrView A, const Epi epi) {
-    grid_dep_launch();
-    grid_dep_wait();
+__device__ __forceinline__ void spmv_fixup_rows(const CsrView& A, const Epi& epi, int tid, int nthreads) {
     typename Epi::State est;
     epi.init(est);
     const AccT* carry = reinterpret_cast<const AccT*>(A.carry);
     const int total = A.num_cross + A.num_empty;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    for (int k = tid; k < total; k += nthreads) {
         if (k < A.num_cross) {
             const int4 c = A.cross[k];   // {row, first tile, tiles, 0}
-            AccT sum = carry[2 * c.y + 1];
-            for (int tt = c.y + 1; tt < c.y + c.z; ++tt) sum += carry[2 * tt];
+            AccT sum = __ldcg(carry + 2 * c.y + 1);
+            for (int tt = c.y + 1; tt < c.y + c.z; ++tt) sum += __ldcg(carry + 2 * tt);
             epi.apply(est, c.x, sum);
         } else {
             epi.apply(est, A.empty_rows[k - A.num_cross], AccT(0));
         }
     }
     epi.finish(est, 1);
+}
+
+template <class Epi, typename AccT>
+__global__ void __launch_bounds__(256)
+    spmv_fixup_kernel(const CsrView A, const Epi epi) {
+    grid_dep_launch();
+    grid_dep_wait();
+    spmv_fixup_rows<Epi, AccT>(A, epi, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -128,6 +128,8 @@ class PdhgOptions:
     use_graph: bool = True
     profile_kernels: bool = False
     refine: bool = True         # adaptive mode: FP64 master iterates + FP32 corrections
+    persistent: int = 0         # Halpern mode: 1 one cooperative kernel per check interval,
+                                # 0 / -1 two dependent launches per iteration in a CUDA graph
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -144,6 +146,7 @@ class PdhgOptions:
         o.use_graph = int(bool(self.use_graph))
         o.profile_kernels = int(bool(self.profile_kernels))
         o.refine = int(bool(self.refine))
+        o.persistent = int(self.persistent)
         return o
 
 

@@ -3,7 +3,7 @@
 Usage:
     python -m pramaan_b200.solve_bench [--lp rolling|random|ill|zipf] [--size A B]
         [--algorithm reference|adaptive|halpern] [--tol 1e-6] [--max-iterations N]
-        [--batch K] [--seed 0]
+        [--batch K] [--seed 0] [--persistent -1|0|1]
 
 `--lp rolling --size T P` is rolling_horizon_lp(T, P); `random --size m n` is
 random_sparse_lp(m, n, 4); `ill --size m n` is ill_conditioned_lp(m, n, 8);
@@ -50,11 +50,12 @@ def main(argv=None):
     ap.add_argument("--check-frequency", type=int, default=64)
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--persistent", type=int, default=0, choices=[-1, 0, 1])
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     algo = {"reference": ALGO_REFERENCE, "adaptive": ALGO_ADAPTIVE, "halpern": ALGO_HALPERN}[a.algorithm]
     o = PdhgOptions(tolerance=a.tol, max_iterations=a.max_iterations, check_frequency=a.check_frequency,
-                    algorithm=algo, device=a.device)
+                    algorithm=algo, device=a.device, persistent=a.persistent)
     if a.batch:
         models = [make(a.lp, *a.size, seed=a.seed + k) for k in range(a.batch)]
         solve_batch(models[:1], o)                 # warm-up (module load)
@@ -72,6 +73,7 @@ def main(argv=None):
         dt = time.perf_counter() - t0
         its, status = r.iterations, r.status.name
     print(json.dumps({"lp": a.lp, "size": list(a.size), "batch": a.batch, "algorithm": a.algorithm,
+                      "persistent": a.persistent,
                       "tol": a.tol, "iterations": its, "status": status, "seconds": dt,
                       "iterations_per_s": its / dt if dt > 0 else None,
                       "us_per_iteration": 1e6 * dt / its if its else None}))

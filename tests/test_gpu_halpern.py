@@ -82,3 +82,29 @@ def test_warm_start_from_the_solution_stops_early():
     warm = solve_batch(models, opts(1e-6), warm=training_targets(cold))
     for c, w in zip(cold, warm):
         assert w.status == SolveStatus.kOptimal and w.iterations <= 64 < c.iterations
+
+
+def test_interval_kernel_matches_the_per_kernel_path_bit_for_bit():
+    """One cooperative kernel per check interval (persistent = 1) computes the
+    same iterates as two launches per iteration in a CUDA graph
+    (persistent = -1): every warp processes the same tiles with the same
+    arithmetic.  The LPs include rows that cross tiles and an empty row, so
+    the in-kernel fixups run."""
+    from pramaan_b200.pdhg import ModelIR
+    with_empty_row = ModelIR([1.0, 2.0, 1.0], [0, 2, 2, 4], [0, 1, 1, 2], [1.0, 1.0, 1.0, -1.0],
+                             [1.0, -1e30, -2.0], [4.0, 5.0, 2.0], [0.0, 0.0, 0.0], [3.0, 3.0, 3.0], 0, 0.0)
+    models = rolling_horizon_batch(5, seed=6, T_range=(24, 60), P_range=(5, 10)) + [
+        random_sparse_lp(300, 900, 4, seed=2), with_empty_row]
+    a = solve_batch(models, PdhgOptions(tolerance=1e-7, max_iterations=200000, check_frequency=64,
+                                        algorithm=ALGO_HALPERN, persistent=1))
+    b = solve_batch(models, PdhgOptions(tolerance=1e-7, max_iterations=200000, check_frequency=64,
+                                        algorithm=ALGO_HALPERN, persistent=-1))
+    for md, ra, rb in zip(models, a, b):
+        assert ra.status == SolveStatus.kOptimal
+        assert ra.iterations == rb.iterations and ra.restarts == rb.restarts
+        assert np.array_equal(ra.x, rb.x) and np.array_equal(ra.y, rb.y)
+    single = PdhgSolver(PdhgOptions(tolerance=1e-7, max_iterations=200000, check_frequency=37,
+                                    algorithm=ALGO_HALPERN, persistent=1)).solve(models[5])
+    single_g = PdhgSolver(PdhgOptions(tolerance=1e-7, max_iterations=200000, check_frequency=37,
+                                      algorithm=ALGO_HALPERN, persistent=-1)).solve(models[5])
+    assert single.iterations == single_g.iterations and np.array_equal(single.x, single_g.x)
