@@ -248,24 +248,47 @@ def _certified(models, results, tol, device):
     return sum(1 for c in cert if c.kkt <= tol * 1.0001)
 
 
-def rolling_horizon_section(args, device):
+def rolling_horizon_section(args, device, dist=None):
     """Batched rolling-horizon LPs (T ~ U{24..336}, P ~ U{5..50}) at 1e-6
-    relative KKT: one packed batch against the same adaptive PDHG solving the
-    LPs one by one (a sample of them)."""
+    relative KKT: one packed batch against the same Halpern PDHG solving the
+    LPs one by one (a sample of them).  With N ranks the batch has N x
+    --rh-count LPs and every rank solves its non-zero-balanced share on its
+    own GPU (no collective on the data path); the time is the maximum over
+    the ranks (weak scaling)."""
+    import torch
+
     from pramaan_b200 import PdhgOptions, PdhgSolver, SolveStatus, solve_batch
+    from pramaan_b200.certificate import certify_batch
     from pramaan_b200.generators import rolling_horizon_batch
+    from pramaan_b200.gnn import WarmStart
+    from pramaan_b200.parallel import shard_plan, solve_batch_sharded
     from pramaan_b200.pdhg import ALGO_HALPERN
 
     tol = 1e-6
+    world = dist.get_world_size() if dist else 1
+    rank = dist.get_rank() if dist else 0
     o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)
-    models = rolling_horizon_batch(args.rh_count, seed=args.seed)
+    models = rolling_horizon_batch(args.rh_count * world, seed=args.seed)
+    mine = shard_plan([m.nnz() for m in models], world)[rank]
     solve_batch(models[:2], o)                       # warm-up (module load, occupancy queries)
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
-    res = solve_batch(models, o)
+    res = solve_batch_sharded(models, o, gather=False)
     tb = time.perf_counter() - t0
-    its = [r.iterations for r in res]
-    idx = np.linspace(0, len(models) - 1, args.rh_plain).astype(int)
+    mres = [res[i] for i in mine]
+    mmod = [models[i] for i in mine]
+    cert = certify_batch(mmod, [[WarmStart(r.x, r.y) for r in mres]], device)[0] if mmod else []
+    counts = torch.tensor([sum(r.status == SolveStatus.kOptimal for r in mres),
+                           sum(1 for c in cert if c.kkt <= tol * 1.0001)], dtype=torch.float64, device=f"cuda:{device}")
+    tmax = torch.tensor([tb], dtype=torch.float64, device=f"cuda:{device}")
+    if dist:
+        dist.all_reduce(counts, op=dist.ReduceOp.SUM)
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tb = float(tmax.item())
+    its = [r.iterations for r in mres]
+    idx = [mine[k] for k in np.linspace(0, len(mine) - 1, min(args.rh_plain, len(mine))).astype(int)]
     solver = PdhgSolver(o)
     plain_t, plain_it = [], []
     for i in idx:
@@ -274,15 +297,16 @@ def rolling_horizon_section(args, device):
         plain_t.append(time.perf_counter() - t0)
         plain_it.append(r.iterations)
     batched = len(models) / tb
-    plain = len(idx) / sum(plain_t)
+    plain = world * len(idx) / sum(plain_t)
     return {"workload": f"rolling_horizon_batch {len(models)} LPs (T~U{{24..336}}, P~U{{5..50}}), "
-                        f"rel KKT {tol:g}, seed {args.seed}; restarted Halpern PDHG, batched and one by one",
+                        f"rel KKT {tol:g}, seed {args.seed}; restarted Halpern PDHG, batched and one by one"
+                        + (f"; {world} ranks, LPs sharded by non-zeros" if world > 1 else ""),
             "rows": sum(m.numRows() for m in models), "cols": sum(m.numVars() for m in models),
             "nnz": sum(m.nnz() for m in models),
-            "batched_lps_per_s": batched, "batched_s": tb, "batched_iterations_median": float(np.median(its)),
-            "optimal": sum(r.status == SolveStatus.kOptimal for r in res),
-            "certified": _certified(models, res, tol, device),
-            "plain_lps_per_s": plain, "plain_sample": int(len(idx)),
+            "batched_lps_per_s": batched, "batched_s": tb,
+            "batched_iterations_median": float(np.median(its)) if its else None,
+            "optimal": int(counts[0].item()), "certified": int(counts[1].item()),
+            "plain_lps_per_s": plain, "plain_sample": int(len(idx)) * world,
             "plain_time_to_tol_median_s": float(np.median(plain_t)),
             "plain_iterations_median": float(np.median(plain_it)),
             "batched_over_plain": batched / plain}
@@ -505,7 +529,7 @@ def run_gpu_arm(args):
 
     if not args.no_rolling:
         line["small_lp"] = small_lp_section(args, local)
-        line["rolling_horizon"] = rolling_horizon_section(args, local)
+        line["rolling_horizon"] = rolling_horizon_section(args, local, dist)
         line["learned_stream"] = learned_stream_section(args, local)
     if rank == 0 and not args.no_cpu_baseline:
         v, threads, sample = cpu_baseline(model, args.cpu_seconds)
