@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--stream-count", type=int, default=32, help="streams of the learned warm-start section")
     p.add_argument("--stream-windows", type=int, default=6, help="windows per stream in that section")
     p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
+    p.add_argument("--gather-cache", type=int, default=0, choices=[0, -1],
+                   help="0: hot gather targets in shared memory (the default); -1: off")
     return p.parse_args()
 
 
@@ -445,8 +447,9 @@ def run_gpu_arm(args):
     torch.cuda.empty_cache()
     nnz = model.nnz()
 
-    opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True)
+    opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True, gather_cache=args.gather_cache)
     sess = Session(model, opts)
+    slots_dual, slots_primal = sess.gather_slots()
     stream = torch.cuda.ExternalStream(sess.stream(), device=local)
     for _ in range(args.warmup):
         sess.iterate(1)
@@ -494,7 +497,9 @@ def run_gpu_arm(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args, nnz), "gpu_launches": int(launches),
+            "config": {**workload_config(args, nnz),
+                       "gather_slots": {"A": slots_dual, "AT": slots_primal}},
+            "gpu_launches": int(launches),
             "clocks": clk.summary(), "roofline": roofline}
 
     # ---- end-to-end through the public C ABI with pinned host buffers ----
@@ -511,7 +516,8 @@ def run_gpu_arm(args):
                                                "row_lower", "row_upper", "var_lower", "var_upper")),
                      model.obj_sense, model.obj_offset)
         solver = pramaan_b200.PdhgSolver(PdhgOptions(device=local, tolerance=0.0,
-                                                     max_iterations=args.e2e_iters, check_frequency=100))
+                                                     max_iterations=args.e2e_iters, check_frequency=100,
+                                                     gather_cache=args.gather_cache))
         solver.solve(pm)   # warm-up (module load, first-touch)
         times = []
         for _ in range(args.e2e_calls):

@@ -107,7 +107,12 @@ typedef struct pramaan_pdhg_options {
                                  products per iteration, captured in a CUDA graph
                                  with dependent launches (faster on the measured
                                  operands)                                      */
-    int32_t reserved[5];
+    int32_t gather_cache;     /* 0 (default): the products over a large operand
+                                 whose gathers concentrate on few entries (the
+                                 transpose of an LP with power-law row lengths)
+                                 keep those entries in shared memory; -1: never.
+                                 The results are identical either way           */
+    int32_t reserved[4];
 } pramaan_pdhg_options;
 
 /* Result, mirroring pramaan::SolveResult (include/pramaan/simplex.hpp:40-76).
@@ -394,6 +399,10 @@ PRAMAAN_API int pramaan_session_kernel_times(pramaan_pdhg_session* s, double* ms
  * notes in the library documentation). */
 PRAMAAN_API int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual,
                                  double* bytes_primal);
+/* Hot gather slots (entries of x kept in shared memory, option gather_cache)
+ * of the dual product's operand A and the primal product's operand A^T. */
+PRAMAAN_API int pramaan_session_gather_slots(pramaan_pdhg_session* s, int32_t* slots_dual,
+                                 int32_t* slots_primal);
 
 #ifdef __cplusplus
 }

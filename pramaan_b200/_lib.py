@@ -36,7 +36,7 @@ class COptions(C.Structure):
         ("tolerance", f64), ("max_iterations", i32), ("check_frequency", i32),
         ("algorithm", i32), ("termination", i32), ("device", i32), ("use_graph", i32),
         ("profile_kernels", i32), ("refine", i32), ("reserved_d", f64),
-        ("persistent", i32), ("reserved", i32 * 5),
+        ("persistent", i32), ("gather_cache", i32), ("reserved", i32 * 4),
     ]
 
 
@@ -118,6 +118,7 @@ SIGNATURES = [
     ("pramaan_session_kernel_times", C.c_int,
      [P, C.POINTER(f64), C.POINTER(f64), C.POINTER(i64), i32]),
     ("pramaan_session_kernel_bytes", C.c_int, [P, C.POINTER(f64), C.POINTER(f64)]),
+    ("pramaan_session_gather_slots", C.c_int, [P, C.POINTER(i32), C.POINTER(i32)]),
 ]
 
 _lib: C.CDLL | None = None

@@ -390,6 +390,14 @@ int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual, do
     });
 }
 
+int pramaan_session_gather_slots(pramaan_pdhg_session* s, int32_t* slots_dual, int32_t* slots_primal) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        if (slots_dual) *slots_dual = s->eng->hot_slots_dual();
+        if (slots_primal) *slots_primal = s->eng->hot_slots_primal();
+    });
+}
+
 // ---- precision ladder ----------------------------------------------------
 
 void pramaan_ladder_default_options(pramaan_ladder_options* opt) {

@@ -511,6 +511,7 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     for (int q = 0; q < K_; ++q) h_action_[q] = kActNone;
 
     preconditioned_steps();          // flat operands: before pack()
+    if (opt_.gather_cache == 0) select_hot_pair(A_, AT_, dev_, st_);
     A_.pack(st_);
     AT_.pack(st_);
     // occupancy queries / shared-memory attributes before any graph capture
@@ -754,7 +755,8 @@ bool AdaptiveBatch::use_interval_kernel() const {
     // only on request: on the measured LPs (60 k and 12 k non-zeros) the
     // graph of dependent launches was faster per iteration (24 / 15 us) than
     // the cooperative kernel with its grid barriers (31 / 21 us)
-    return halpern_ && m_ > 0 && opt_.persistent > 0;
+    // (the cooperative kernel reads the operands without hot gather slots)
+    return halpern_ && m_ > 0 && opt_.persistent > 0 && A_.hot == 0 && AT_.hot == 0;
 }
 
 void AdaptiveBatch::launch_interval(int k) {
@@ -1266,6 +1268,7 @@ void AdaptiveBatch::compact() {
         PB_CUDA_CHECK(cudaMemsetAsync(flag.get(), 0, 4, st_));
         csr_upload_f64(nA, nm, nn, nnz, rp.data(), ci.data(), val.data(), st_, flag.get());
         csr_transpose(nA, nAT, st_);
+        if (opt_.gather_cache == 0) select_hot_pair(nA, nAT, dev_, st_);
         nA.pack(st_);
         nAT.pack(st_);
         autotune_operand(nA, st_, dev_, status_.get());

@@ -175,10 +175,11 @@ __global__ void keys_to_rowptr_kernel(const int* __restrict__ keys, int nnz, int
     }
 }
 
-// One block per tile: interleave the flat arrays into the tile record.
+// One block per tile: interleave the flat arrays into the tile record; an
+// entry whose target has a hot slot stores ~slot.
 __global__ void pack_kernel(const int* __restrict__ col, const float* __restrict__ val,
                             const uint32_t* __restrict__ flags, const int4* __restrict__ meta,
-                            int tiles, unsigned char* __restrict__ rec) {
+                            const int* __restrict__ slot, int tiles, unsigned char* __restrict__ rec) {
     constexpr int TW = TileRec::TW, FW = TileRec::FW;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
         unsigned char* r = rec + size_t(t) * TileRec::bytes;
@@ -187,7 +188,12 @@ __global__ void pack_kernel(const int* __restrict__ col, const float* __restrict
         uint32_t* rf = reinterpret_cast<uint32_t*>(r + TileRec::off_flags);
         const size_t base = size_t(t) * TW;
         for (int k = threadIdx.x; k < TW; k += blockDim.x) {
-            rc[k] = col[base + k];
+            int c = col[base + k];
+            if (slot) {
+                const int h = slot[c];
+                if (h >= 0) c = ~h;
+            }
+            rc[k] = c;
             rv[k] = val[base + k];
         }
         for (int k = threadIdx.x; k < FW; k += blockDim.x) rf[k] = flags[size_t(t) * FW + k];
@@ -207,18 +213,76 @@ __global__ void permute_kernel(const int* __restrict__ perm, const int* __restri
     }
 }
 
+__global__ void target_counts_kernel(const int* __restrict__ rp, int n, int* __restrict__ counts,
+                                     int* __restrict__ ids) {
+    PB_GRID_STRIDE(i, n) {
+        counts[i] = rp[i + 1] - rp[i];
+        ids[i] = int(i);
+    }
+}
+
+__global__ void slot_scatter_kernel(const int* __restrict__ ids, int H, int* __restrict__ slot) {
+    PB_GRID_STRIDE(k, H) slot[ids[k]] = int(k);
+}
+
 }  // namespace
+
+void CsrDevice::select_hot(const int* target_rp, int num_targets, int dev, cudaStream_t st) {
+    hot = 0;
+    hot_idx.reset();
+    hot_slot.reset();
+    if (packed || num_tiles == 0 || num_targets <= 0 || target_rp == nullptr) return;
+    using Launch = SpmvLauncher<EpiStore<float, float>, float, float, false>;
+    const int sms = device_sm_count(dev);
+    // Each block of the hot kernel copies every slot once, so an operand with
+    // few tiles per block gains nothing.
+    const long long blocks = (long long)sms * Launch::kHotTargetBlocks;
+    if ((long long)num_tiles < 64 * blocks * kSpmvHotWarps / 8) return;
+    const int n = num_targets;
+    DevBuf<int> counts{size_t(n)}, ids{size_t(n)}, counts_s{size_t(n)}, ids_s{size_t(n)};
+    target_counts_kernel<<<grid_1d(n), kThreads, 0, st>>>(target_rp, n, counts.get(), ids.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    size_t tb = 0;
+    PB_CUDA_CHECK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, counts.get(), counts_s.get(), ids.get(),
+                                                            ids_s.get(), n, 0, 32, st));
+    DevBuf<unsigned char> temp(tb > 0 ? tb : 1);
+    PB_CUDA_CHECK(cub::DeviceRadixSort::SortPairsDescending(temp.get(), tb, counts.get(), counts_s.get(), ids.get(),
+                                                            ids_s.get(), n, 0, 32, st));
+    const int H0 = n < kSpmvHotCap ? n : kSpmvHotCap;
+    std::vector<int> hc(static_cast<size_t>(H0));
+    PB_CUDA_CHECK(cudaMemcpyAsync(hc.data(), counts_s.get(), size_t(H0) * 4, cudaMemcpyDeviceToHost, st));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    const long long min_uses = (long long)kSpmvHotMinUses * blocks;
+    long long covered = 0;
+    int H = 0;
+    while (H < H0 && (long long)hc[size_t(H)] >= min_uses) covered += hc[size_t(H++)];
+    if (H == 0 || double(covered) < kSpmvHotMinShare * double(nnz)) return;
+    hot_idx.alloc(size_t(H));
+    PB_CUDA_CHECK(cudaMemcpyAsync(hot_idx.get(), ids_s.get(), size_t(H) * 4, cudaMemcpyDeviceToDevice, st));
+    hot_slot.alloc(size_t(n));
+    PB_CUDA_CHECK(cudaMemsetAsync(hot_slot.get(), 0xff, hot_slot.bytes(), st));   // -1: no slot
+    slot_scatter_kernel<<<grid_1d(H), kThreads, 0, st>>>(ids_s.get(), H, hot_slot.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));   // temporaries are freed on return
+    hot = H;
+}
+
+void select_hot_pair(CsrDevice& A, CsrDevice& AT, int dev, cudaStream_t st) {
+    AT.select_hot(A.row_ptr.get(), A.rows, dev, st);
+    A.select_hot(AT.row_ptr.get(), AT.rows, dev, st);
+}
 
 void CsrDevice::pack(cudaStream_t st) {
     if (packed) return;
     if (num_tiles > 0) {
         rec.alloc(size_t(num_tiles) * TileRec::bytes);
         const int grid = num_tiles < 65535 * 4 ? num_tiles : 65535 * 4;
-        pack_kernel<<<grid, 256, 0, st>>>(col.get(), val.get(), flags.get(), meta.get(), num_tiles,
-                                          rec.get());
+        pack_kernel<<<grid, 256, 0, st>>>(col.get(), val.get(), flags.get(), meta.get(),
+                                          hot > 0 ? hot_slot.get() : nullptr, num_tiles, rec.get());
         PB_CUDA_CHECK(cudaGetLastError());
         PB_CUDA_CHECK(cudaStreamSynchronize(st));
     }
+    hot_slot.reset();
     col.reset();
     val.reset();
     flags.reset();
@@ -229,6 +293,9 @@ void CsrDevice::pack(cudaStream_t st) {
 void CsrDevice::allocate(int rows_, int cols_, int nnz_, bool lo) {
     if (rows_ < 0 || cols_ < 0 || nnz_ < 0) throw InvalidArgument("negative CSR dimension");
     rows = rows_; cols = cols_; nnz = nnz_;
+    hot = 0;
+    hot_idx.reset();
+    hot_slot.reset();
     num_tiles = nnz > 0 ? ceil_div(nnz, kSpmvTile) : 0;
     nnz_pad = num_tiles * kSpmvTile;
     has_lo = lo;
@@ -413,7 +480,7 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status) {
     using Epi = EpiStore<float, float>;
     using Launch = SpmvLauncher<Epi, float, float, false>;
     if (A.num_tiles < 4 * device_sm_count(dev)) return;   // small operands: default grid
-    const int occ = Launch::blocks_per_sm(dev);
+    const int occ = A.hot > 0 ? Launch::hot_blocks_per_sm(dev) : Launch::blocks_per_sm(dev);
     DevBuf<float> xs(static_cast<size_t>(A.cols > 0 ? A.cols : 1)), ys(static_cast<size_t>(A.rows));
     PB_CUDA_CHECK(cudaMemsetAsync(xs.get(), 0, xs.bytes(), st));
     Epi epi{ys.get()};

@@ -15,6 +15,8 @@
 //   empty_rows int32 [rows - rows_c]   rows without entries
 //   cross      int4  [crossing rows]   {row, first tile, tiles, 0} per row spanning tiles
 //   carry      f64   [2 * tiles]       per-tile partials of crossing rows (scratch)
+//   hot_idx    int32 [hot]             gather target of every hot slot (records
+//                                      hold ~slot for those entries; see spmv.cuh)
 // nnz_pad is a multiple of the tile (512 entries); records are 4176 bytes and
 // every array starts on a 256-byte boundary (cudaMalloc), so each record and
 // each tile's val_lo slab is 16-byte aligned for the bulk copies.  While an
@@ -75,9 +77,10 @@ public:
     int rows = 0, cols = 0, nnz = 0, nnz_pad = 0, num_tiles = 0;
     int rows_c = 0, num_empty = 0, num_cross = 0;
     int tuned_blocks_per_sm = 0;   // set by the launch autotuner (0: default)
+    int hot = 0;                   // hot gather slots
     bool has_lo = false;
     bool packed = false;
-    DevBuf<int> row_ptr, col, row_map, empty_rows;
+    DevBuf<int> row_ptr, col, row_map, empty_rows, hot_idx, hot_slot;
     DevBuf<float> val, val_lo;
     DevBuf<uint32_t> flags;
     DevBuf<int4> meta, cross;
@@ -94,6 +97,7 @@ public:
         v.val_lo = (with_lo && has_lo) ? val_lo.get() : nullptr;
         v.row_map = row_map.get(); v.empty_rows = empty_rows.get();
         v.cross = cross.get(); v.carry = carry.get();
+        v.hot = hot; v.hot_idx = hot_idx.get();
         return v;
     }
 
@@ -108,10 +112,19 @@ public:
     void allocate(int rows_, int cols_, int nnz_, bool lo);
     // Builds flags / meta / row compaction / crossing rows from row_ptr.
     void finalize(cudaStream_t st);
-    // Interleaves col / val / flags / meta into tile records and frees them.
+    // Interleaves col / val / flags / meta into tile records and frees them
+    // (entries whose target has a hot slot get ~slot).
     void pack(cudaStream_t st);
+    // Chooses the hot gather targets before pack(): `target_rp` is the row
+    // pointer of the operand whose rows are this operand's gather targets
+    // (A's for AT, AT's for A), so target i is gathered target_rp[i+1] -
+    // target_rp[i] times.  A target gets a slot when it is gathered at least
+    // kSpmvHotMinUses times per resident block of the hot kernel (each block
+    // loads every slot once); the slots are kept only when they take at least
+    // kSpmvHotMinShare of the non-zeros.  No-op for small operands.
+    void select_hot(const int* target_rp, int num_targets, int dev, cudaStream_t st);
     size_t device_bytes() const {
-        return row_ptr.bytes() + col.bytes() + row_map.bytes() + empty_rows.bytes() +
+        return row_ptr.bytes() + col.bytes() + row_map.bytes() + empty_rows.bytes() + hot_idx.bytes() +
                val.bytes() + val_lo.bytes() + flags.bytes() + meta.bytes() + cross.bytes() +
                rec.bytes() + carry.bytes();
     }
@@ -129,6 +142,8 @@ void csr_upload_f32(CsrDevice& A, int rows, int cols, int nnz, const int* h_row_
 // increasing order, the order of the reference's counting-sort transpose,
 // src/linalg/sparse_matrix.cpp:13-57).
 void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st);
+// Hot gather slots for both operands of a product pair (before pack()).
+void select_hot_pair(CsrDevice& A, CsrDevice& AT, int dev, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // Launch helpers
@@ -142,6 +157,15 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status);
 
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
+// Hot-slot kernel: one block per SM of kSpmvHotWarps warps (aliased staging,
+// ~92 KB) plus the 64 KB FP32 hot copy, which keeps the 164 KB shared-memory
+// carve-out and so ~92 KB of L1 for the outstanding cold gathers.  Measured on
+// the 2,000,000 x 5,000,000 Zipf LP: 8 warps 0.548 ms, 11 warps 0.459 ms, 14
+// warps with an 8 K-slot copy 0.459 ms, no hot slots 0.505 ms per A^T y.
+constexpr int kSpmvHotWarps = 11;
+constexpr int kSpmvHotCap = 16384;            // most hot slots
+constexpr int kSpmvHotMinUses = 2;            // gathers per slot per resident block
+constexpr double kSpmvHotMinShare = 0.15;     // share of the non-zeros the slots must take
 
 // Launches `k` with programmatic stream serialization, so that it may start
 // while the previous kernel of the stream finishes (the kernels wait with
@@ -168,6 +192,21 @@ struct SpmvLauncher {
     static constexpr auto kernel() {
         return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvWarps, kSpmvStages>;
     }
+    // Operands with hot slots: FP32 gathers use the shared-memory copy (kHot
+    // 1, kSpmvHotWarps warps per block); wider gathers resolve the slots
+    // through hot_idx with the plain layout (kHot 2).
+    static constexpr int kHotMode = sizeof(XT) == 4 ? 1 : 2;
+    static constexpr int kHotWarps = kHotMode == 1 ? kSpmvHotWarps : kSpmvWarps;
+    using LH = SpmvSmemLayout<kHotWarps, kSpmvStages, kLo, AccT, kHotMode == 1>;
+    static constexpr size_t kHotSmem = LH::bytes + (kHotMode == 1 ? size_t(kSpmvHotCap) * sizeof(XT) : 0);
+    template <bool kRowMap>
+    static constexpr auto hot_kernel() {
+        return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kHotWarps, kSpmvStages, kHotMode>;
+    }
+    // Resident blocks per SM the hot kernel is configured for.
+    static constexpr int kHotTargetBlocks =
+        kHotMode == 1 ? (int((228 * 1024) / (kHotSmem + 1024)) > 0 ? int((228 * 1024) / (kHotSmem + 1024)) : 1)
+                      : (int((132 * 1024) / (L::bytes + 1024)) > 0 ? int((132 * 1024) / (L::bytes + 1024)) : 1);
     // Default resident blocks per SM: as many as fit in ~132 KB of shared
     // memory, which leaves ~100 KB of L1 for outstanding gather misses.
     static constexpr int kTargetBlocks =
@@ -194,21 +233,54 @@ struct SpmvLauncher {
         cache[dev].store(nb, std::memory_order_relaxed);
         return nb;
     }
-    // Queries occupancy (and sets the shared-memory attributes) for both
+    template <bool kRowMap>
+    static int hot_blocks_per_sm_impl(int dev) {
+        static std::atomic<int> cache[64];
+        if (dev < 0 || dev >= 64) dev = 0;
+        int v = cache[dev].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+        PB_CUDA_CHECK(cudaFuncSetAttribute(hot_kernel<kRowMap>(),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(kHotSmem)));
+        const long long need = (long long)kHotTargetBlocks * (kHotSmem + 1024);
+        int pct = int((need * 100 + 228 * 1024 - 1) / (228 * 1024));
+        pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+        PB_CUDA_CHECK(cudaFuncSetAttribute(hot_kernel<kRowMap>(),
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        int nb = 0;
+        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, hot_kernel<kRowMap>(),
+                                                                    kHotWarps * 32, kHotSmem));
+        if (nb < 1) nb = 1;
+        cache[dev].store(nb, std::memory_order_relaxed);
+        return nb;
+    }
+    // Queries occupancy (and sets the shared-memory attributes) for all
     // variants; call before any stream capture.
     static int blocks_per_sm(int dev) {
         blocks_per_sm_impl<true>(dev);
+        hot_blocks_per_sm_impl<true>(dev);
+        hot_blocks_per_sm_impl<false>(dev);
         return blocks_per_sm_impl<false>(dev);
+    }
+    static int hot_blocks_per_sm(int dev) {
+        hot_blocks_per_sm_impl<true>(dev);
+        return hot_blocks_per_sm_impl<false>(dev);
     }
     // Grid for one launch: A.blocks_per_sm (autotuned) or the default target,
     // never more than fit, never more blocks than tile groups.
+    // For an operand with hot slots the tuned value applies to the FP32 hot
+    // kernel (the one the tuner times); the kHot 2 kernels use the default.
     static int grid_for(const CsrView& A, int dev) {
         const bool mapped = A.row_map != nullptr;
-        const int occ = mapped ? blocks_per_sm_impl<true>(dev) : blocks_per_sm_impl<false>(dev);
-        int bps = A.blocks_per_sm > 0 ? A.blocks_per_sm : kTargetBlocks;
+        const bool hot = A.hot > 0;
+        const int occ = hot ? (mapped ? hot_blocks_per_sm_impl<true>(dev) : hot_blocks_per_sm_impl<false>(dev))
+                            : (mapped ? blocks_per_sm_impl<true>(dev) : blocks_per_sm_impl<false>(dev));
+        int bps;
+        if (hot) bps = (kHotMode == 1 && A.blocks_per_sm > 0) ? A.blocks_per_sm : kHotTargetBlocks;
+        else bps = A.blocks_per_sm > 0 ? A.blocks_per_sm : kTargetBlocks;
         bps = bps < occ ? bps : occ;
+        const int warps = hot ? kHotWarps : kSpmvWarps;
         const long long cap = (long long)bps * device_sm_count(dev);
-        const long long need = (A.num_tiles + kSpmvWarps - 1) / kSpmvWarps;
+        const long long need = (A.num_tiles + warps - 1) / warps;
         return int(need < cap ? need : cap);
     }
     static void launch(const CsrView& A, const XT* x, const Epi& epi, int* dev_status,
@@ -217,10 +289,17 @@ struct SpmvLauncher {
         if (A.num_tiles > 0) {
             const bool mapped = A.row_map != nullptr;
             const int grid = grid_for(A, dev);
-            if (mapped)
+            if (A.hot > 0) {
+                if (A.hot > kSpmvHotCap || A.hot_idx == nullptr) throw std::logic_error("SpmvLauncher: bad hot slots");
+                if (mapped)
+                    launch_dependent(hot_kernel<true>(), grid, kHotWarps * 32, kHotSmem, st, A, x, epi, dev_status);
+                else
+                    launch_dependent(hot_kernel<false>(), grid, kHotWarps * 32, kHotSmem, st, A, x, epi, dev_status);
+            } else if (mapped) {
                 launch_dependent(kernel<true>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
-            else
+            } else {
                 launch_dependent(kernel<false>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
+            }
         }
         const int fix = A.num_cross + A.num_empty;
         if (fix > 0) {

@@ -50,6 +50,8 @@ public:
     void kernel_times(double* ms_dual, double* ms_primal, long long* launches, bool reset);
     double bytes_dual() const;
     double bytes_primal() const;
+    int hot_slots_dual() const { return A_.hot; }
+    int hot_slots_primal() const { return AT_.hot; }
     void synchronize();
 
     // ---- adaptive mode (pdhg_adaptive.cu) ----

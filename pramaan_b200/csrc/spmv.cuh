@@ -23,6 +23,16 @@
 //   alone: row(q) = first_row + #starts in (0, q].  The kernel never reads
 //   row_ptr.
 //
+// Hot gather targets
+//   When a few x entries take a large share of the gathers (the transpose of
+//   an LP with power-law row lengths: every entry of a long row of A gathers
+//   the same y), the operand lists them as hot slots (hot_idx[slot] = target)
+//   and its records hold ~slot (a negative index) for those entries.  The
+//   FP32 kernels copy the hot targets into shared memory once per block and
+//   read them from there, so only the cold gathers reach L2; other kernels
+//   resolve ~slot through hot_idx.  The value gathered, and so every sum, is
+//   the same either way.
+//
 // What bounds it
 //   On a random sparsity pattern every entry costs one 4-byte gather of x
 //   from L2, and B200 serves random gathers at about one L1 request per clock
@@ -90,9 +100,51 @@ struct CsrView {
     const int* empty_rows = nullptr;  // num_empty
     const int4* cross = nullptr;      // num_cross: {original row, first tile, tiles, 0}
     void* carry = nullptr;            // 2 * num_tiles accumulators (8-byte slots)
+    int hot = 0;                      // hot gather slots (records hold ~slot for them)
+    const int* hot_idx = nullptr;     // hot: gather target of every slot
 };
 
-template <int WARPS, int STAGES, bool kLo, typename AccT>
+// Predicated ld.global.cg: the load is issued only when `pred` holds, so hot
+// lanes send no request at all (pointing them all at one address instead
+// concentrates the requests of every SM on one L2 slice: measured 2x slower).
+// The address must be valid either way; callers pass an in-range one.  Not
+// volatile: the compiler may schedule it like an ordinary load.
+__device__ __forceinline__ float ldcg_if(const float* p, bool pred) {
+    float v = 0.f;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q ld.global.cg.f32 %0, [%1];\n\t}"
+        : "+f"(v) : "l"(p), "r"(int(pred)));
+    return v;
+}
+__device__ __forceinline__ double ldcg_if(const double* p, bool pred) {
+    double v = 0.0;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q ld.global.cg.f64 %0, [%1];\n\t}"
+        : "+d"(v) : "l"(p), "r"(int(pred)));
+    return v;
+}
+
+// Gather of entry index c (kHot 0: plain; 1: ~slot from the block's shared
+// copy `hs`; 2: ~slot resolved through hot_idx).  Every address formed is in
+// range whichever way the selects go.
+template <int kHot, typename XT>
+__device__ __forceinline__ XT spmv_gather(const XT* __restrict__ x, const XT* hs, const CsrView& A, int c) {
+    if constexpr (kHot == 1) {
+        const bool cold = c >= 0;
+        const XT g = ldcg_if(x + (cold ? c : 0), cold);
+        const XT h = hs[cold ? 0 : ~c];
+        return cold ? g : h;
+    } else if constexpr (kHot == 2) {
+        const int t = __ldg(A.hot_idx + (c >= 0 ? 0 : ~c));
+        return __ldcg(x + (c >= 0 ? c : t));
+    } else {
+        return __ldcg(x + c);
+    }
+}
+
+// kAlias: the finished-row values of a tile are staged over the tile's own
+// column / value slots (every lane has moved those to registers by then), so
+// a warp needs no shared memory beyond its ring.  Used by the hot-slot
+// kernel, whose block also holds the hot copy: the saving buys it warps.
+template <int WARPS, int STAGES, bool kLo, typename AccT, bool kAlias = false>
 struct SpmvSmemLayout {
     static constexpr int TW = kSpmvTile;
     static constexpr int FW = TileRec::FW;
@@ -101,8 +153,11 @@ struct SpmvSmemLayout {
     static constexpr size_t off_meta = TileRec::off_meta;
     static constexpr size_t off_lo = TileRec::bytes;                         // kLo only
     static constexpr size_t stage_bytes = TileRec::bytes + (kLo ? size_t(TW) * 4 : 0);
-    static constexpr size_t off_fin = size_t(STAGES) * stage_bytes;        // finished-row values
-    static constexpr size_t warp_bytes = (off_fin + size_t(TW) * sizeof(AccT) + 15) / 16 * 16;
+    static constexpr size_t off_fin = size_t(STAGES) * stage_bytes;        // finished-row values (no alias)
+    static constexpr size_t warp_bytes =
+        kAlias ? (off_fin + 15) / 16 * 16 : (off_fin + size_t(TW) * sizeof(AccT) + 15) / 16 * 16;
+    static_assert(!kAlias || size_t(TW) * sizeof(AccT) <= off_flags,
+                  "staged row values must fit in the column / value slots");
     static constexpr size_t off_bar = size_t(WARPS) * warp_bytes;
     static constexpr size_t bytes = ((off_bar + size_t(WARPS) * STAGES * 8) + 127) / 128 * 128;
     static constexpr unsigned tx_bytes = unsigned(stage_bytes);
@@ -132,11 +187,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // written: a grid dependency wait, or a grid barrier in a multi-product
 // kernel; it returns false to abandon the product.  Returns false when a wait
 // gave up (the status word records it).
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, class Ready>
+// kHot (see spmv_gather): with 1 the block's copy of the hot targets sits
+// after the rings (shared-memory offset L::bytes, A.hot values of XT).
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kHot = 0,
+          class Ready>
 __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restrict__ x, const Epi& epi,
                                            int* __restrict__ dev_status, unsigned char* smem, uint32_t& used,
                                            bool init_bars, Ready&& ready) {
-    using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT>;
+    constexpr bool kAlias = kHot == 1;
+    using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT, kAlias>;
     constexpr int IPT = kSpmvIpt;
     constexpr int TW = L::TW;
     constexpr int FW = L::FW;
@@ -145,7 +204,8 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     unsigned char* ring = smem + size_t(warp) * L::warp_bytes;
-    AccT* fin = reinterpret_cast<AccT*>(ring + L::off_fin);
+    // staged row values: a per-warp buffer, or (aliased) the current stage, set per tile
+    AccT* fin = kAlias ? nullptr : reinterpret_cast<AccT*>(ring + L::off_fin);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::off_bar) + warp * STAGES;
 
     const int rows_c = A.rows_c;
@@ -188,6 +248,27 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
     // carry[] are touched only once ready() has returned.
     bool failed = !ready();
 
+    XT* hs = reinterpret_cast<XT*>(smem + L::bytes);
+    if constexpr (kHot == 1) {
+        __syncthreads();   // an earlier product of the same kernel may still read the copy
+        const int H = A.hot;
+        constexpr int U = 8;
+        for (int k0 = threadIdx.x; k0 < H; k0 += WARPS * 32 * U) {
+            XT v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + u * WARPS * 32;
+                v[u] = k < H ? __ldcg(x + __ldg(A.hot_idx + k)) : XT(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + u * WARPS * 32;
+                if (k < H) hs[k] = v[u];
+            }
+        }
+        __syncthreads();
+    }
+
     AccT* carry = reinterpret_cast<AccT*>(A.carry);
     int i = 0;
     for (; i < mine && !failed; ++i) {
@@ -218,13 +299,18 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
             const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
             // ld.global.cg: the gathers are served by L2; caching them in L1
             // only evicts lines other warps are waiting on.
-            xv[j] = __ldcg(x + c4.x); xv[j + 1] = __ldcg(x + c4.y);
-            xv[j + 2] = __ldcg(x + c4.z); xv[j + 3] = __ldcg(x + c4.w);
+            xv[j] = spmv_gather<kHot>(x, hs, A, c4.x); xv[j + 1] = spmv_gather<kHot>(x, hs, A, c4.y);
+            xv[j + 2] = spmv_gather<kHot>(x, hs, A, c4.z); xv[j + 3] = spmv_gather<kHot>(x, hs, A, c4.w);
             vv[j] = v4.x; vv[j + 1] = v4.y; vv[j + 2] = v4.z; vv[j + 3] = v4.w;
             if constexpr (kLo) {
                 const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
                 ll[j] = l4.x; ll[j + 1] = l4.y; ll[j + 2] = l4.z; ll[j + 3] = l4.w;
             }
+        }
+        if constexpr (kAlias) {
+            // every lane holds its columns and values now: the slots take the staged rows
+            __syncwarp();
+            fin = reinterpret_cast<AccT*>(const_cast<unsigned char*>(st));
         }
 
         // ---- row-start bits of my entries and of the entry after them ----
@@ -333,13 +419,14 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
     return !failed;
 }
 
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES>
-__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS)
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kHot = 0>
+__global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS > 0
+                                                  ? (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS : 1)
     spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
                      int* __restrict__ dev_status) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t used = 0;
-    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES>(A, x, epi, dev_status, smem, used, true, [] {
+    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES, kHot>(A, x, epi, dev_status, smem, used, true, [] {
         grid_dep_launch();
         grid_dep_wait();
         return true;

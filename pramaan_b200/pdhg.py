@@ -130,6 +130,7 @@ class PdhgOptions:
     refine: bool = True         # adaptive mode: FP64 master iterates + FP32 corrections
     persistent: int = 0         # Halpern mode: 1 one cooperative kernel per check interval,
                                 # 0 / -1 two dependent launches per iteration in a CUDA graph
+    gather_cache: int = 0       # 0: hot gather targets of large skewed operands in shared memory; -1: off
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -147,6 +148,7 @@ class PdhgOptions:
         o.profile_kernels = int(bool(self.profile_kernels))
         o.refine = int(bool(self.refine))
         o.persistent = int(self.persistent)
+        o.gather_cache = int(self.gather_cache)
         return o
 
 
@@ -370,4 +372,11 @@ class Session:
     def kernel_bytes(self) -> tuple[float, float]:
         a, b = C.c_double(), C.c_double()
         L.check(L.lib().pramaan_session_kernel_bytes(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def gather_slots(self) -> tuple[int, int]:
+        """Hot gather slots of the dual product's operand A and the primal
+        product's operand A^T (0: no shared-memory gather cache)."""
+        a, b = C.c_int32(), C.c_int32()
+        L.check(L.lib().pramaan_session_gather_slots(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value

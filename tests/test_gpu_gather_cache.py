@@ -1,0 +1,66 @@
+"""Shared-memory gather cache (hot gather slots of an operand).
+
+On an LP with power-law row lengths the transpose's gathers concentrate on
+the long rows' y entries; the products keep those entries in shared memory.
+The value gathered is the same either way, so every iterate must be
+bit-identical with the cache on (option gather_cache 0) and off (-1), in the
+reference iteration (FP32 products, FP64 residual products with the FP32
+remainders) and in the Halpern mode (FP64 master gathers through the slot
+table).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from pramaan_b200 import PdhgOptions, PdhgSolver
+from pramaan_b200 import generators as gen
+from pramaan_b200.pdhg import ALGO_HALPERN, ALGO_REFERENCE, Session
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def zipf_mid():
+    # ~10.8 M non-zeros: large enough for the cache, rows Zipf(1.5) up to 5,000 long
+    return gen.zipf_lp(200_000, 500_000, seed=3, device="cuda")
+
+
+def test_reference_iterates_identical_with_and_without_cache(zipf_mid):
+    runs = {}
+    for cache in (0, -1):
+        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+                        gather_cache=cache)
+        with Session(zipf_mid, o) as s:
+            slots = s.gather_slots()
+            s.iterate(60)
+            res = s.residuals()
+            x, y = s.iterates()
+        runs[cache] = (slots, res, x, y)
+    slots_on, res_on, x_on, y_on = runs[0]
+    slots_off, res_off, x_off, y_off = runs[-1]
+    assert slots_off == (0, 0)
+    assert slots_on[0] == 0             # columns are uniform: no hot targets in A
+    assert 1000 < slots_on[1] <= 16384  # the long rows' y entries in A^T
+    assert np.array_equal(x_on, x_off) and np.array_equal(y_on, y_off)
+    assert res_on == res_off
+    assert np.isfinite(x_on).all() and np.abs(y_on).max() > 0
+
+
+def test_halpern_solve_identical_with_and_without_cache(zipf_mid):
+    out = {}
+    for cache in (0, -1):
+        o = PdhgOptions(tolerance=1e-12, max_iterations=640, check_frequency=64, algorithm=ALGO_HALPERN,
+                        gather_cache=cache)
+        out[cache] = PdhgSolver(o).solve(zipf_mid)
+    a, b = out[0], out[-1]
+    assert a.iterations == b.iterations
+    assert a.status == b.status
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+    assert a.objective_value == b.objective_value
+
+
+def test_gather_cache_option_is_validated():
+    md = gen.random_sparse_lp(50, 120, 4, seed=1)
+    with pytest.raises(ValueError):
+        PdhgSolver(PdhgOptions(gather_cache=1)).solve(md)
