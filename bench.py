@@ -15,6 +15,10 @@ Lines printed (rank 0, one JSON line):
              buffers: upload, 1000 iterations (checks every 100), download
   roofline   the dominant product kernel's algorithmic bytes / CUDA-event time
   cpu_baseline  the oracle's multi-threaded FP32 iteration on the host cores
+  banded_spmv   the same iteration on a banded LP of the same size (local
+             gathers): per-kernel GB/s against the measured HBM bandwidth
+  small_lp, rolling_horizon, learned_stream   the plain-PDHG LP, the batched
+             rolling-horizon LPs and the learned warm start (see each section)
 
 `--impl reference` times the reference algorithm's CPU restatement (the
 oracle; the reference has no CPU implementation of this path) on all host
@@ -62,8 +66,11 @@ def parse():
     p.add_argument("--stream-count", type=int, default=32, help="streams of the learned warm-start section")
     p.add_argument("--stream-windows", type=int, default=6, help="windows per stream in that section")
     p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
-    p.add_argument("--gather-cache", type=int, default=0, choices=[0, -1],
-                   help="0: hot gather targets in shared memory (the default); -1: off")
+    p.add_argument("--no-banded", action="store_true", help="skip the banded-LP bandwidth section")
+    p.add_argument("--banded-iters", type=int, default=50)
+    p.add_argument("--gather-cache", type=int, default=0, choices=[0, 1, -1],
+                   help="0: hot gather targets in shared memory, L1-cached gathers where faster (the "
+                        "default); 1: L1-cached gathers wherever there are no hot slots; -1: plain")
     return p.parse_args()
 
 
@@ -406,6 +413,50 @@ def small_lp_section(args, device):
     return out
 
 
+def banded_section(args, device):
+    """The same iteration on a banded LP of the headline size (2,000,000 x
+    5,000,000, 54 columns per row within +-256 of i*n/m): local gathers, so the
+    products can run at the HBM roofline.  Device-timed per-kernel bandwidth
+    (algorithmic bytes over CUDA-event time) with the autotuner's gather mode
+    and with plain L2 gathers."""
+    import torch
+
+    from pramaan_b200 import PdhgOptions
+    from pramaan_b200.generators import banded_lp, model_from_tensors
+    from pramaan_b200.pdhg import Session
+
+    t = banded_lp(args.m, args.n, per_row=54, band=256, seed=args.seed, device=f"cuda:{device}", as_tensors=True)
+    model = model_from_tensors(t)
+    del t
+    torch.cuda.empty_cache()
+    hbm, kind = measured_peaks()
+    out = {"workload": f"banded_lp {args.m} x {args.n}, 54 per row, band 256, seed {args.seed}",
+           "nnz": int(model.nnz()), "peak_gbs": hbm, "peak_kind": kind, "iterations": args.banded_iters}
+    for name, cache in (("auto", 0), ("l2_gathers", -1)):
+        with Session(model, PdhgOptions(device=device, use_graph=False, profile_kernels=True,
+                                        gather_cache=cache)) as sess:
+            for _ in range(3):
+                sess.iterate(1)
+            sess.synchronize()
+            sess.kernel_times(reset=True)
+            stream = torch.cuda.ExternalStream(sess.stream(), device=device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.banded_iters):
+                sess.iterate(1)
+            e1.record(stream)
+            e1.synchronize()
+            ms_dual, ms_primal, _ = sess.kernel_times(reset=True)
+            b_dual, b_primal = sess.kernel_bytes()
+            k = args.banded_iters
+            res = {"iterations_per_s": k / (e0.elapsed_time(e1) / 1000.0), "gather": sess.gather_info()}
+            for tag, ms, by in (("dual", ms_dual, b_dual), ("primal", ms_primal, b_primal)):
+                gbs = by / (ms / 1000.0 / k) / 1e9
+                res[tag] = {"avg_launch_ms": ms / k, "achieved_gbs": gbs, "frac": gbs / hbm}
+            out[name] = res
+    return out
+
+
 def _hints_for(batch, prev):
     """Each stream's previous window solution shifted onto its current window."""
     from pramaan_b200 import SolveStatus
@@ -449,7 +500,7 @@ def run_gpu_arm(args):
 
     opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True, gather_cache=args.gather_cache)
     sess = Session(model, opts)
-    slots_dual, slots_primal = sess.gather_slots()
+    gather = sess.gather_info()
     stream = torch.cuda.ExternalStream(sess.stream(), device=local)
     for _ in range(args.warmup):
         sess.iterate(1)
@@ -498,7 +549,7 @@ def run_gpu_arm(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**workload_config(args, nnz),
-                       "gather_slots": {"A": slots_dual, "AT": slots_primal}},
+                       "gather": gather},
             "gpu_launches": int(launches),
             "clocks": clk.summary(), "roofline": roofline}
 
@@ -533,6 +584,8 @@ def run_gpu_arm(args):
                        "iterations_per_call": args.e2e_iters, "calls": args.e2e_calls,
                        "call_s_median": statistics.median(times)}
 
+    if not args.no_banded:
+        line["banded_spmv"] = banded_section(args, local)
     if not args.no_rolling:
         line["small_lp"] = small_lp_section(args, local)
         line["rolling_horizon"] = rolling_horizon_section(args, local, dist)

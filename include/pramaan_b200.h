@@ -110,8 +110,13 @@ typedef struct pramaan_pdhg_options {
     int32_t gather_cache;     /* 0 (default): the products over a large operand
                                  whose gathers concentrate on few entries (the
                                  transpose of an LP with power-law row lengths)
-                                 keep those entries in shared memory; -1: never.
-                                 The results are identical either way           */
+                                 keep those entries in shared memory, and the
+                                 launch autotuner caches the gathers of the
+                                 other large operands in L1 where that is
+                                 faster (local column patterns); 1: as 0, but
+                                 L1-cached gathers on every operand without hot
+                                 entries; -1: plain L2 gathers only.  The
+                                 results are identical in every mode            */
     int32_t reserved[4];
 } pramaan_pdhg_options;
 
@@ -399,10 +404,12 @@ PRAMAAN_API int pramaan_session_kernel_times(pramaan_pdhg_session* s, double* ms
  * notes in the library documentation). */
 PRAMAAN_API int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual,
                                  double* bytes_primal);
-/* Hot gather slots (entries of x kept in shared memory, option gather_cache)
- * of the dual product's operand A and the primal product's operand A^T. */
-PRAMAAN_API int pramaan_session_gather_slots(pramaan_pdhg_session* s, int32_t* slots_dual,
-                                 int32_t* slots_primal);
+/* Gather modes (option gather_cache) of the dual product's operand A and the
+ * primal product's operand A^T: hot gather slots (entries of x kept in shared
+ * memory) and whether the gathers are cached in L1 (1) or not (0).  Any
+ * pointer may be NULL. */
+PRAMAAN_API int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual,
+                                int32_t* slots_primal, int32_t* l1_dual, int32_t* l1_primal);
 
 #ifdef __cplusplus
 }

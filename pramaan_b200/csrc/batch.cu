@@ -511,7 +511,7 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     for (int q = 0; q < K_; ++q) h_action_[q] = kActNone;
 
     preconditioned_steps();          // flat operands: before pack()
-    if (opt_.gather_cache == 0) select_hot_pair(A_, AT_, dev_, st_);
+    if (opt_.gather_cache >= 0) select_hot_pair(A_, AT_, dev_, st_);
     A_.pack(st_);
     AT_.pack(st_);
     // occupancy queries / shared-memory attributes before any graph capture
@@ -524,8 +524,8 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     warm_launcher<EpiStore<double, double>, double, double>(dev_);
     warm_launcher<EpiRowViolOut, double, double>(dev_);
     warm_launcher<EpiColResidOut, double, double>(dev_);
-    autotune_operand(A_, st_, dev_, status_.get());
-    autotune_operand(AT_, st_, dev_, status_.get());
+    autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache);
+    autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache);
     estimate_step_sizes();
 
     // initial primal weight per LP: ||C c|| / ||R b|| on the scaled LP
@@ -1268,11 +1268,11 @@ void AdaptiveBatch::compact() {
         PB_CUDA_CHECK(cudaMemsetAsync(flag.get(), 0, 4, st_));
         csr_upload_f64(nA, nm, nn, nnz, rp.data(), ci.data(), val.data(), st_, flag.get());
         csr_transpose(nA, nAT, st_);
-        if (opt_.gather_cache == 0) select_hot_pair(nA, nAT, dev_, st_);
+        if (opt_.gather_cache >= 0) select_hot_pair(nA, nAT, dev_, st_);
         nA.pack(st_);
         nAT.pack(st_);
-        autotune_operand(nA, st_, dev_, status_.get());
-        autotune_operand(nAT, st_, dev_, status_.get());
+        autotune_operand(nA, st_, dev_, status_.get(), opt_.gather_cache);
+        autotune_operand(nAT, st_, dev_, status_.get(), opt_.gather_cache);
     }
 
     // 4. the first compaction keeps the original layout for the final evaluation

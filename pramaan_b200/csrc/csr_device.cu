@@ -473,14 +473,19 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st) {
     AT.finalize(st);   // synchronises; temporaries are freed on return
 }
 
-// Launch autotuner: picks the resident blocks per SM for one operand by
-// timing the SpMV (store-only epilogue into scratch, so no iterate changes)
-// at every candidate occupancy, and records the fastest in the operand.
-void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status) {
+// Launch autotuner: picks the resident blocks per SM and the gather mode for
+// one operand by timing the SpMV (store-only epilogue into scratch, so no
+// iterate changes) for every candidate, and records the fastest in the operand.
+void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache) {
     using Epi = EpiStore<float, float>;
     using Launch = SpmvLauncher<Epi, float, float, false>;
+    A.gather_l1 = (gather_cache > 0 && A.hot == 0) ? 1 : 0;
     if (A.num_tiles < 4 * device_sm_count(dev)) return;   // small operands: default grid
     const int occ = A.hot > 0 ? Launch::hot_blocks_per_sm(dev) : Launch::blocks_per_sm(dev);
+    // L1-cached gathers are a candidate for operands without hot slots; the
+    // L2 mode is timed first and kept unless the other is 2 % faster.
+    const int mode_lo = A.gather_l1;
+    const int mode_hi = (gather_cache == 0 && A.hot == 0) ? 1 : A.gather_l1;
     DevBuf<float> xs(static_cast<size_t>(A.cols > 0 ? A.cols : 1)), ys(static_cast<size_t>(A.rows));
     PB_CUDA_CHECK(cudaMemsetAsync(xs.get(), 0, xs.bytes(), st));
     Epi epi{ys.get()};
@@ -488,22 +493,26 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status) {
     PB_CUDA_CHECK(cudaEventCreate(&e0));
     PB_CUDA_CHECK(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_bps = 0;
-    for (int bps = 1; bps <= occ && bps <= 4; ++bps) {
-        A.tuned_blocks_per_sm = bps;
-        const CsrView v = A.view(false);
-        Launch::launch(v, xs.get(), epi, status, st, dev);   // warm-up
-        PB_CUDA_CHECK(cudaEventRecord(e0, st));
-        for (int r = 0; r < 3; ++r) Launch::launch(v, xs.get(), epi, status, st, dev);
-        PB_CUDA_CHECK(cudaEventRecord(e1, st));
-        PB_CUDA_CHECK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        PB_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best * 0.98f) { best = ms; best_bps = bps; }
+    int best_bps = 0, best_mode = mode_lo;
+    for (int mode = mode_lo; mode <= mode_hi; ++mode) {
+        for (int bps = 1; bps <= occ && bps <= 4; ++bps) {
+            A.tuned_blocks_per_sm = bps;
+            A.gather_l1 = mode;
+            const CsrView v = A.view(false);
+            Launch::launch(v, xs.get(), epi, status, st, dev);   // warm-up
+            PB_CUDA_CHECK(cudaEventRecord(e0, st));
+            for (int r = 0; r < 3; ++r) Launch::launch(v, xs.get(), epi, status, st, dev);
+            PB_CUDA_CHECK(cudaEventRecord(e1, st));
+            PB_CUDA_CHECK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PB_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best * 0.98f) { best = ms; best_bps = bps; best_mode = mode; }
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     A.tuned_blocks_per_sm = best_bps;
+    A.gather_l1 = best_mode;
 }
 
 

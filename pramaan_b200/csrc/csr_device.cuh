@@ -78,6 +78,7 @@ public:
     int rows_c = 0, num_empty = 0, num_cross = 0;
     int tuned_blocks_per_sm = 0;   // set by the launch autotuner (0: default)
     int hot = 0;                   // hot gather slots
+    int gather_l1 = 0;             // gathers cached in L1 (set by the launch autotuner)
     bool has_lo = false;
     bool packed = false;
     DevBuf<int> row_ptr, col, row_map, empty_rows, hot_idx, hot_slot;
@@ -98,6 +99,7 @@ public:
         v.row_map = row_map.get(); v.empty_rows = empty_rows.get();
         v.cross = cross.get(); v.carry = carry.get();
         v.hot = hot; v.hot_idx = hot_idx.get();
+        v.gather_l1 = gather_l1;
         return v;
     }
 
@@ -151,9 +153,12 @@ void select_hot_pair(CsrDevice& A, CsrDevice& AT, int dev, cudaStream_t st);
 int device_sm_count(int dev);
 
 // Launch autotuner: times the store-only product of `A` at 1-4 resident
-// blocks per SM and records the fastest in A.tuned_blocks_per_sm (operands
-// with fewer than 4 tiles per SM keep the default grid).
-void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status);
+// blocks per SM and, for an operand without hot slots, with L2 and with
+// L1-cached gathers, and records the fastest in A.tuned_blocks_per_sm and
+// A.gather_l1 (operands with fewer than 4 tiles per SM keep the default grid
+// and L2 gathers).  gather_cache is the option of that name: -1 keeps L2
+// gathers, 1 takes L1-cached gathers without timing them, 0 times both.
+void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache);
 
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
@@ -192,43 +197,48 @@ struct SpmvLauncher {
     static constexpr auto kernel() {
         return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvWarps, kSpmvStages>;
     }
-    // Operands with hot slots: FP32 gathers use the shared-memory copy (kHot
-    // 1, kSpmvHotWarps warps per block); wider gathers resolve the slots
-    // through hot_idx with the plain layout (kHot 2).
-    static constexpr int kHotMode = sizeof(XT) == 4 ? 1 : 2;
-    static constexpr int kHotWarps = kHotMode == 1 ? kSpmvHotWarps : kSpmvWarps;
-    using LH = SpmvSmemLayout<kHotWarps, kSpmvStages, kLo, AccT, kHotMode == 1>;
-    static constexpr size_t kHotSmem = LH::bytes + (kHotMode == 1 ? size_t(kSpmvHotCap) * sizeof(XT) : 0);
+    template <bool kRowMap>
+    static constexpr auto l1_kernel() {
+        return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvWarps, kSpmvStages, kGatherL1>;
+    }
+    // Operands with hot slots: FP32 gathers use the shared-memory copy
+    // (kGatherHot, kSpmvHotWarps warps per block); wider gathers resolve the
+    // slots through hot_idx with the plain layout (kGatherHotIdx).
+    static constexpr int kHotMode = sizeof(XT) == 4 ? kGatherHot : kGatherHotIdx;
+    static constexpr int kHotWarps = kHotMode == kGatherHot ? kSpmvHotWarps : kSpmvWarps;
+    using LH = SpmvSmemLayout<kHotWarps, kSpmvStages, kLo, AccT, kHotMode == kGatherHot>;
+    static constexpr size_t kHotSmem =
+        LH::bytes + (kHotMode == kGatherHot ? size_t(kSpmvHotCap) * sizeof(XT) : 0);
     template <bool kRowMap>
     static constexpr auto hot_kernel() {
         return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kHotWarps, kSpmvStages, kHotMode>;
     }
     // Resident blocks per SM the hot kernel is configured for.
     static constexpr int kHotTargetBlocks =
-        kHotMode == 1 ? (int((228 * 1024) / (kHotSmem + 1024)) > 0 ? int((228 * 1024) / (kHotSmem + 1024)) : 1)
+        kHotMode == kGatherHot
+            ? (int((228 * 1024) / (kHotSmem + 1024)) > 0 ? int((228 * 1024) / (kHotSmem + 1024)) : 1)
                       : (int((132 * 1024) / (L::bytes + 1024)) > 0 ? int((132 * 1024) / (L::bytes + 1024)) : 1);
     // Default resident blocks per SM: as many as fit in ~132 KB of shared
     // memory, which leaves ~100 KB of L1 for outstanding gather misses.
     static constexpr int kTargetBlocks =
         int((132 * 1024) / (L::bytes + 1024)) > 0 ? int((132 * 1024) / (L::bytes + 1024)) : 1;
 
-    template <bool kRowMap>
+    // kL1: the L1-cached variant (same layout and carve-out as the plain one).
+    template <bool kRowMap, bool kL1 = false>
     static int blocks_per_sm_impl(int dev) {
         static std::atomic<int> cache[64];
         if (dev < 0 || dev >= 64) dev = 0;
         int v = cache[dev].load(std::memory_order_relaxed);
         if (v > 0) return v;
-        PB_CUDA_CHECK(cudaFuncSetAttribute(kernel<kRowMap>(),
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes)));
+        const auto k = kL1 ? l1_kernel<kRowMap>() : kernel<kRowMap>();
+        PB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::bytes)));
         // Carve-out for kTargetBlocks blocks (percent of the 228 KB maximum).
         const long long need = (long long)kTargetBlocks * (L::bytes + 1024);
         int pct = int((need * 100 + 228 * 1024 - 1) / (228 * 1024));
         pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
-        PB_CUDA_CHECK(cudaFuncSetAttribute(kernel<kRowMap>(),
-                                           cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        PB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         int nb = 0;
-        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel<kRowMap>(),
-                                                                    kSpmvWarps * 32, L::bytes));
+        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kSpmvWarps * 32, L::bytes));
         if (nb < 1) nb = 1;
         cache[dev].store(nb, std::memory_order_relaxed);
         return nb;
@@ -257,6 +267,8 @@ struct SpmvLauncher {
     // variants; call before any stream capture.
     static int blocks_per_sm(int dev) {
         blocks_per_sm_impl<true>(dev);
+        blocks_per_sm_impl<true, true>(dev);
+        blocks_per_sm_impl<false, true>(dev);
         hot_blocks_per_sm_impl<true>(dev);
         hot_blocks_per_sm_impl<false>(dev);
         return blocks_per_sm_impl<false>(dev);
@@ -275,7 +287,7 @@ struct SpmvLauncher {
         const int occ = hot ? (mapped ? hot_blocks_per_sm_impl<true>(dev) : hot_blocks_per_sm_impl<false>(dev))
                             : (mapped ? blocks_per_sm_impl<true>(dev) : blocks_per_sm_impl<false>(dev));
         int bps;
-        if (hot) bps = (kHotMode == 1 && A.blocks_per_sm > 0) ? A.blocks_per_sm : kHotTargetBlocks;
+        if (hot) bps = (kHotMode == kGatherHot && A.blocks_per_sm > 0) ? A.blocks_per_sm : kHotTargetBlocks;
         else bps = A.blocks_per_sm > 0 ? A.blocks_per_sm : kTargetBlocks;
         bps = bps < occ ? bps : occ;
         const int warps = hot ? kHotWarps : kSpmvWarps;
@@ -295,6 +307,11 @@ struct SpmvLauncher {
                     launch_dependent(hot_kernel<true>(), grid, kHotWarps * 32, kHotSmem, st, A, x, epi, dev_status);
                 else
                     launch_dependent(hot_kernel<false>(), grid, kHotWarps * 32, kHotSmem, st, A, x, epi, dev_status);
+            } else if (A.gather_l1) {
+                if (mapped)
+                    launch_dependent(l1_kernel<true>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
+                else
+                    launch_dependent(l1_kernel<false>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
             } else if (mapped) {
                 launch_dependent(kernel<true>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);
             } else {

@@ -120,7 +120,7 @@ void validate_options(const pramaan_pdhg_options& opt) {
                               "error (PRAMAAN_TERM_RELATIVE_KKT)");
     if (opt.refine != 0 && opt.refine != 1) throw InvalidArgument("pdhg options: refine must be 0 or 1");
     if (opt.persistent < -1 || opt.persistent > 1) throw InvalidArgument("pdhg options: persistent must be -1, 0 or 1");
-    if (opt.gather_cache < -1 || opt.gather_cache > 0) throw InvalidArgument("pdhg options: gather_cache must be -1 or 0");
+    if (opt.gather_cache < -1 || opt.gather_cache > 1) throw InvalidArgument("pdhg options: gather_cache must be -1, 0 or 1");
     if (opt.algorithm == PRAMAAN_ALGO_HALPERN && opt.refine != 1)
         throw InvalidArgument("pdhg options: the Halpern algorithm runs on FP64 master iterates (refine = 1)");
 }
@@ -193,7 +193,7 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     // (they also read the flat operands).
     if (opt.algorithm == PRAMAAN_ALGO_ADAPTIVE) setup_adaptive(lp);
     // The step sizes above read the flat operands; interleave them into tile records now.
-    if (opt.gather_cache == 0) select_hot_pair(A_, AT_, dev_, st_);
+    if (opt.gather_cache >= 0) select_hot_pair(A_, AT_, dev_, st_);
     A_.pack(st_);
     AT_.pack(st_);
     // Occupancy queries / smem attributes before any graph capture.
@@ -207,8 +207,8 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     SpmvLauncher<EpiStore<float, float>, float, float, false>::blocks_per_sm(dev_);
     // The FP32 product kernels share one shared-memory layout, so the grid the
     // tuner picks for the store-only kernel carries over to the PDHG epilogues.
-    autotune_operand(A_, st_, dev_, status_.get());
-    autotune_operand(AT_, st_, dev_, status_.get());
+    autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache);
+    autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache);
     if (adaptive_) {
         SpmvLauncher<EpiDualAdapt, float, float, false>::blocks_per_sm(dev_);
         SpmvLauncher<EpiPrimalAdapt, float, float, false>::blocks_per_sm(dev_);

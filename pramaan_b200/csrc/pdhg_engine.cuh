@@ -52,6 +52,8 @@ public:
     double bytes_primal() const;
     int hot_slots_dual() const { return A_.hot; }
     int hot_slots_primal() const { return AT_.hot; }
+    int gather_l1_dual() const { return A_.gather_l1; }
+    int gather_l1_primal() const { return AT_.gather_l1; }
     void synchronize();
 
     // ---- adaptive mode (pdhg_adaptive.cu) ----

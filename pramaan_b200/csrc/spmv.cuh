@@ -33,6 +33,13 @@
 //   resolve ~slot through hot_idx.  The value gathered, and so every sum, is
 //   the same either way.
 //
+// Local gathers
+//   The default gathers (ld.global.cg) skip L1: on a random pattern caching
+//   them only evicts lines other warps wait on.  When an operand's columns are
+//   local (banded and multi-period structures), ld.global.ca lets neighbouring
+//   rows reuse the lines in L1; the launch autotuner times both and records
+//   the faster in the operand (gather_l1).
+//
 // What bounds it
 //   On a random sparsity pattern every entry costs one 4-byte gather of x
 //   from L2, and B200 serves random gathers at about one L1 request per clock
@@ -102,7 +109,14 @@ struct CsrView {
     void* carry = nullptr;            // 2 * num_tiles accumulators (8-byte slots)
     int hot = 0;                      // hot gather slots (records hold ~slot for them)
     const int* hot_idx = nullptr;     // hot: gather target of every slot
+    int gather_l1 = 0;                // gathers cached in L1 (operands without hot slots)
 };
+
+// Gather modes of the product kernel.
+constexpr int kGatherL2 = 0;       // ld.global.cg
+constexpr int kGatherHot = 1;      // ~slot from the block's shared copy, the rest ld.global.cg
+constexpr int kGatherHotIdx = 2;   // ~slot resolved through hot_idx
+constexpr int kGatherL1 = 3;       // ld.global.ca
 
 // Predicated ld.global.cg: the load is issued only when `pred` holds, so hot
 // lanes send no request at all (pointing them all at one address instead
@@ -122,19 +136,20 @@ __device__ __forceinline__ double ldcg_if(const double* p, bool pred) {
     return v;
 }
 
-// Gather of entry index c (kHot 0: plain; 1: ~slot from the block's shared
-// copy `hs`; 2: ~slot resolved through hot_idx).  Every address formed is in
-// range whichever way the selects go.
-template <int kHot, typename XT>
+// Gather of entry index c in mode kG (hs: the block's shared copy of the hot
+// targets).  Every address formed is in range whichever way the selects go.
+template <int kG, typename XT>
 __device__ __forceinline__ XT spmv_gather(const XT* __restrict__ x, const XT* hs, const CsrView& A, int c) {
-    if constexpr (kHot == 1) {
+    if constexpr (kG == kGatherHot) {
         const bool cold = c >= 0;
         const XT g = ldcg_if(x + (cold ? c : 0), cold);
         const XT h = hs[cold ? 0 : ~c];
         return cold ? g : h;
-    } else if constexpr (kHot == 2) {
+    } else if constexpr (kG == kGatherHotIdx) {
         const int t = __ldg(A.hot_idx + (c >= 0 ? 0 : ~c));
         return __ldcg(x + (c >= 0 ? c : t));
+    } else if constexpr (kG == kGatherL1) {
+        return __ldca(x + c);
     } else {
         return __ldcg(x + c);
     }
@@ -187,14 +202,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // written: a grid dependency wait, or a grid barrier in a multi-product
 // kernel; it returns false to abandon the product.  Returns false when a wait
 // gave up (the status word records it).
-// kHot (see spmv_gather): with 1 the block's copy of the hot targets sits
-// after the rings (shared-memory offset L::bytes, A.hot values of XT).
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kHot = 0,
+// kG: gather mode (spmv_gather).  With kGatherHot the block's copy of the
+// hot targets sits after the rings (shared-memory offset L::bytes, A.hot
+// values of XT).
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kG = kGatherL2,
           class Ready>
 __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restrict__ x, const Epi& epi,
                                            int* __restrict__ dev_status, unsigned char* smem, uint32_t& used,
                                            bool init_bars, Ready&& ready) {
-    constexpr bool kAlias = kHot == 1;
+    constexpr bool kAlias = kG == kGatherHot;
     using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT, kAlias>;
     constexpr int IPT = kSpmvIpt;
     constexpr int TW = L::TW;
@@ -249,7 +265,7 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
     bool failed = !ready();
 
     XT* hs = reinterpret_cast<XT*>(smem + L::bytes);
-    if constexpr (kHot == 1) {
+    if constexpr (kG == kGatherHot) {
         __syncthreads();   // an earlier product of the same kernel may still read the copy
         const int H = A.hot;
         constexpr int U = 8;
@@ -299,8 +315,8 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
             const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
             // ld.global.cg: the gathers are served by L2; caching them in L1
             // only evicts lines other warps are waiting on.
-            xv[j] = spmv_gather<kHot>(x, hs, A, c4.x); xv[j + 1] = spmv_gather<kHot>(x, hs, A, c4.y);
-            xv[j + 2] = spmv_gather<kHot>(x, hs, A, c4.z); xv[j + 3] = spmv_gather<kHot>(x, hs, A, c4.w);
+            xv[j] = spmv_gather<kG>(x, hs, A, c4.x); xv[j + 1] = spmv_gather<kG>(x, hs, A, c4.y);
+            xv[j + 2] = spmv_gather<kG>(x, hs, A, c4.z); xv[j + 3] = spmv_gather<kG>(x, hs, A, c4.w);
             vv[j] = v4.x; vv[j + 1] = v4.y; vv[j + 2] = v4.z; vv[j + 3] = v4.w;
             if constexpr (kLo) {
                 const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
@@ -419,14 +435,14 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
     return !failed;
 }
 
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kHot = 0>
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kG = kGatherL2>
 __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS > 0
                                                   ? (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS : 1)
     spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
                      int* __restrict__ dev_status) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t used = 0;
-    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES, kHot>(A, x, epi, dev_status, smem, used, true, [] {
+    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES, kG>(A, x, epi, dev_status, smem, used, true, [] {
         grid_dep_launch();
         grid_dep_wait();
         return true;

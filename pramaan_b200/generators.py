@@ -125,6 +125,18 @@ def zipf_lp(m: int = 2_000_000, n: int = 5_000_000, s: float = 1.5, cap: int = 5
     counts = torch.bincount(rows, minlength=m)
     row_ptr = torch.zeros(m + 1, dtype=torch.int64, device=dev)
     torch.cumsum(counts, 0, out=row_ptr[1:])
+    return _lp_on_structure(rows, cols, row_ptr, m, n, g, dev, scale_lo, scale_hi, as_tensors)
+
+
+def _lp_on_structure(rows, cols, row_ptr, m, n, g, dev, scale_lo, scale_hi, as_tensors):
+    """Values, a feasible point and bounded costs on a given structure (torch
+    tensors: rows int64 and cols int32 per entry in CSR order, row_ptr int64).
+    Values FP32(N(0,1) * row scale), row scales log-uniform in
+    [scale_lo, scale_hi]; b = A x0 with x0 ~ U(0,1) in [0, ub]; c = A^T y0 + s0
+    with s0 > 0, so the LP is feasible and bounded."""
+    import torch
+
+    nnz = cols.numel()
     lo, hi = np.log10(scale_lo), np.log10(scale_hi)
     rscale = torch.pow(10.0, lo + (hi - lo) * torch.rand(m, generator=g, dtype=torch.float64, device=dev))
     vals = (torch.randn(nnz, generator=g, dtype=torch.float64, device=dev) * rscale[rows]).float().double()
@@ -143,6 +155,41 @@ def zipf_lp(m: int = 2_000_000, n: int = 5_000_000, s: float = 1.5, cap: int = 5
     h = {k2: v.cpu().numpy() for k2, v in t.items()}
     return ModelIR(h["obj_coeffs"], h["row_ptr"], h["col_idx"], h["values"], h["row_lower"],
                    h["row_upper"], h["var_lower"], h["var_upper"], ObjSense.kMinimize, 0.0)
+
+
+def banded_lp(m: int = 2_000_000, n: int = 5_000_000, per_row: int = 54, band: int = 256, seed: int = 0,
+              scale_lo: float = 1e-2, scale_hi: float = 1e2, device: str = "cpu", as_tensors: bool = False):
+    """LP whose rows couple nearby columns (torch on `device`).
+
+    Row i draws `per_row` columns uniformly within +-band of i*n/m (clamped to
+    [0, n); duplicates merged, so the actual nnz is reported by the result):
+    the locally coupled structure of multi-period and network models ordered
+    by period or node.  Values, bounds and costs as zipf_lp.  Returns a
+    ModelIR (host) or, with as_tensors=True, a dict of torch tensors.
+    """
+    import torch
+
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    rows = torch.arange(m, device=dev).repeat_interleave(per_row)
+    center = torch.div(rows * n, m, rounding_mode="floor")
+    cols = (center + torch.randint(-band, band + 1, (rows.numel(),), generator=g, device=dev)).clamp_(0, n - 1)
+    del center
+    key = rows * n + cols
+    del rows, cols
+    key, _ = torch.sort(key)
+    keep = torch.ones_like(key, dtype=torch.bool)
+    keep[1:] = key[1:] != key[:-1]
+    key = key[keep]
+    del keep
+    rows = torch.div(key, n, rounding_mode="floor")
+    cols = (key - rows * n).to(torch.int32)
+    del key
+    counts = torch.bincount(rows, minlength=m)
+    row_ptr = torch.zeros(m + 1, dtype=torch.int64, device=dev)
+    torch.cumsum(counts, 0, out=row_ptr[1:])
+    return _lp_on_structure(rows, cols, row_ptr, m, n, g, dev, scale_lo, scale_hi, as_tensors)
 
 
 def model_from_tensors(t: dict) -> ModelIR:

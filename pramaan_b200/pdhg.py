@@ -130,7 +130,9 @@ class PdhgOptions:
     refine: bool = True         # adaptive mode: FP64 master iterates + FP32 corrections
     persistent: int = 0         # Halpern mode: 1 one cooperative kernel per check interval,
                                 # 0 / -1 two dependent launches per iteration in a CUDA graph
-    gather_cache: int = 0       # 0: hot gather targets of large skewed operands in shared memory; -1: off
+    gather_cache: int = 0       # 0: hot gather targets of large skewed operands in shared memory and
+                                # L1-cached gathers where the autotuner finds them faster;
+                                # 1: L1-cached gathers on every operand without hot slots; -1: plain
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -374,9 +376,16 @@ class Session:
         L.check(L.lib().pramaan_session_kernel_bytes(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def gather_info(self) -> dict:
+        """Gather modes of the dual product's operand A and the primal
+        product's operand A^T: hot gather slots (0: no shared-memory copy) and
+        whether the gathers are cached in L1."""
+        v = [C.c_int32() for _ in range(4)]
+        L.check(L.lib().pramaan_session_gather_info(self._h, *(C.byref(q) for q in v)))
+        return {"A": {"hot_slots": v[0].value, "l1": bool(v[2].value)},
+                "AT": {"hot_slots": v[1].value, "l1": bool(v[3].value)}}
+
     def gather_slots(self) -> tuple[int, int]:
-        """Hot gather slots of the dual product's operand A and the primal
-        product's operand A^T (0: no shared-memory gather cache)."""
-        a, b = C.c_int32(), C.c_int32()
-        L.check(L.lib().pramaan_session_gather_slots(self._h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+        """Hot gather slots of A and A^T."""
+        g = self.gather_info()
+        return g["A"]["hot_slots"], g["AT"]["hot_slots"]

@@ -2,8 +2,10 @@
 
 On an LP with power-law row lengths the transpose's gathers concentrate on
 the long rows' y entries; the products keep those entries in shared memory.
-The value gathered is the same either way, so every iterate must be
-bit-identical with the cache on (option gather_cache 0) and off (-1), in the
+Operands with local columns may instead have their gathers cached in L1.
+The value gathered is the same in every mode, so every iterate must be
+bit-identical with the option gather_cache at 0 (automatic), 1 (L1-cached
+gathers wherever there are no hot slots) and -1 (plain L2 gathers), in the
 reference iteration (FP32 products, FP64 residual products with the FP32
 remainders) and in the Halpern mode (FP64 master gathers through the slot
 table).
@@ -63,4 +65,41 @@ def test_halpern_solve_identical_with_and_without_cache(zipf_mid):
 def test_gather_cache_option_is_validated():
     md = gen.random_sparse_lp(50, 120, 4, seed=1)
     with pytest.raises(ValueError):
-        PdhgSolver(PdhgOptions(gather_cache=1)).solve(md)
+        PdhgSolver(PdhgOptions(gather_cache=2)).solve(md)
+
+
+@pytest.fixture(scope="module")
+def banded_mid():
+    # ~10.7 M non-zeros, every row's columns within +-256 of i*n/m: local gathers, no hot targets
+    return gen.banded_lp(400_000, 1_000_000, per_row=27, band=256, seed=2, device="cuda")
+
+
+def test_l1_cached_gathers_identical_to_l2_gathers(banded_mid):
+    runs = {}
+    for cache in (1, 0, -1):
+        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+                        gather_cache=cache)
+        with Session(banded_mid, o) as s:
+            info = s.gather_info()
+            s.iterate(40)
+            res = s.residuals()
+            x, y = s.iterates()
+        runs[cache] = (info, res, x, y)
+    forced, auto, off = runs[1], runs[0], runs[-1]
+    assert forced[0]["A"] == {"hot_slots": 0, "l1": True} and forced[0]["AT"] == {"hot_slots": 0, "l1": True}
+    assert off[0]["A"] == {"hot_slots": 0, "l1": False} and off[0]["AT"] == {"hot_slots": 0, "l1": False}
+    assert auto[0]["A"]["hot_slots"] == 0 and auto[0]["AT"]["hot_slots"] == 0
+    for run in (forced, auto):
+        assert np.array_equal(run[2], off[2]) and np.array_equal(run[3], off[3])
+        assert run[1] == off[1]
+
+
+def test_halpern_with_hot_slots_and_l1_gathers_identical(zipf_mid):
+    out = {}
+    for cache in (1, -1):
+        o = PdhgOptions(tolerance=1e-12, max_iterations=320, check_frequency=64, algorithm=ALGO_HALPERN,
+                        gather_cache=cache)
+        out[cache] = PdhgSolver(o).solve(zipf_mid)
+    a, b = out[1], out[-1]
+    assert a.iterations == b.iterations
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
