@@ -193,8 +193,8 @@ __global__ void pack_kernel(const int* __restrict__ col, const float* __restrict
                 const int h = slot[c];
                 if (h >= 0) c = ~h;
             }
-            rc[k] = c;
-            rv[k] = val[base + k];
+            rc[tile_slot(k)] = c;
+            rv[tile_slot(k)] = val[base + k];
         }
         for (int k = threadIdx.x; k < FW; k += blockDim.x) rf[k] = flags[size_t(t) * FW + k];
         if (threadIdx.x == 0) *reinterpret_cast<int4*>(r + TileRec::off_meta) = meta[t];
@@ -210,6 +210,15 @@ __global__ void permute_kernel(const int* __restrict__ perm, const int* __restri
         t_col[k] = row_of[src];
         t_val[k] = val[src];
         if (t_lo) t_lo[k] = lo[src];
+    }
+}
+
+// The FP32 remainders in the records' lane-interleaved order (tile_slot).
+__global__ void interleave_lo_kernel(const float* __restrict__ src, long long n, float* __restrict__ dst) {
+    PB_GRID_STRIDE(i, n) {
+        const long long t = i / kSpmvTile;
+        const int q = int(i - t * kSpmvTile);
+        dst[t * kSpmvTile + tile_slot(q)] = src[i];
     }
 }
 
@@ -280,6 +289,14 @@ void CsrDevice::pack(cudaStream_t st) {
         pack_kernel<<<grid, 256, 0, st>>>(col.get(), val.get(), flags.get(), meta.get(),
                                           hot > 0 ? hot_slot.get() : nullptr, num_tiles, rec.get());
         PB_CUDA_CHECK(cudaGetLastError());
+        if (has_lo && val_lo.get()) {
+            DevBuf<float> lo_i{size_t(nnz_pad)};
+            interleave_lo_kernel<<<grid_1d(nnz_pad), kThreads, 0, st>>>(val_lo.get(), (long long)nnz_pad,
+                                                                        lo_i.get());
+            PB_CUDA_CHECK(cudaGetLastError());
+            PB_CUDA_CHECK(cudaStreamSynchronize(st));
+            val_lo = std::move(lo_i);
+        }
         PB_CUDA_CHECK(cudaStreamSynchronize(st));
     }
     hot_slot.reset();

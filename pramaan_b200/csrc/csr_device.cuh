@@ -5,11 +5,14 @@
 //   row_ptr    int32 [rows + 1]        the CSR row pointer as given
 //   rec        tile records [tiles]    per tile: col int32[512] (pad: 0),
 //                                      val fp32[512] (FP32-rounded, pad: 0),
+//                                      both lane-interleaved (tile_slot),
 //                                      flags u32[16] (bit q: entry q starts a
 //                                      non-empty row), meta int4
 //                                      {first_row, tail_continues, 0, 0}
 //   val_lo     fp32  [nnz_pad]         FP32(value - val), kept only when some
-//                                      value is not exactly representable
+//                                      value is not exactly representable (entry
+//                                      order while building, tile_slot order
+//                                      once packed)
 //   row_map    int32 [rows_c]          original row of each non-empty row (only
 //                                      when empty rows exist)
 //   empty_rows int32 [rows - rows_c]   rows without entries

@@ -11,8 +11,8 @@
 //   tile per warp at a time.  Each tile is ONE contiguous record, so a single
 //   ~4 KB bulk copy moves it (copies of 2 KB or less stream at well under
 //   half of HBM bandwidth on B200; 4 KB and up reach it):
-//     col   int32[TW]     column indices
-//     val   fp32 [TW]     values (FP32-rounded)
+//     col   int32[TW]     column indices  (lane-interleaved, see tile_slot)
+//     val   fp32 [TW]     values (FP32-rounded, same order)
 //     flags u32 [TW/32]   bit q set <=> entry q starts a row
 //     meta  int4          {first_row, tail_continues, 0, 0}
 //   The FP32 remainders val_lo (value - val), when present, stay in a flat
@@ -79,6 +79,18 @@ namespace pb {
 
 constexpr int kSpmvIpt = 16;                 // entries per lane
 constexpr int kSpmvTile = 32 * kSpmvIpt;     // entries per warp-tile (format unit)
+
+// Slot of tile-local entry q in a record's column and value arrays (and in
+// the tile's val_lo slab).  Lane l owns entries IPT*l .. IPT*l + IPT-1 and
+// reads them as 16-byte chunks; chunk k of lane l is stored at chunk index
+// k*32 + l, so each chunk read of a warp is 512 contiguous bytes of shared
+// memory (4 wavefronts) instead of 32 reads at a 64-byte stride (16).
+__host__ __device__ constexpr int tile_slot(int q) {
+    return (((q % kSpmvIpt) / 4) * 32 + q / kSpmvIpt) * 4 + (q % 4);
+}
+
+static_assert(tile_slot(0) == 0 && tile_slot(4) == 128 && tile_slot(16) == 4 && tile_slot(511) == 511,
+              "tile_slot layout");
 
 // Byte layout of one tile record.
 struct TileRec {
@@ -298,9 +310,9 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
             break;
         }
         const unsigned char* st = ring + size_t(s) * L::stage_bytes;
-        const int* scol = reinterpret_cast<const int*>(st);
-        const float* sval = reinterpret_cast<const float*>(st + L::off_val);
-        const float* slo = reinterpret_cast<const float*>(st + L::off_lo);
+        const int4* scol4 = reinterpret_cast<const int4*>(st);                  // tile_slot order
+        const float4* sval4 = reinterpret_cast<const float4*>(st + L::off_val);
+        const float4* slo4 = reinterpret_cast<const float4*>(st + L::off_lo);
         const uint32_t* fl = reinterpret_cast<const uint32_t*>(st + L::off_flags);
         const int4 meta = *reinterpret_cast<const int4*>(st + L::off_meta);
         const int q0 = lane * IPT;   // tile-local index of my first entry
@@ -311,15 +323,15 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
         float ll[IPT];
 #pragma unroll
         for (int j = 0; j < IPT; j += 4) {
-            const int4 c4 = *reinterpret_cast<const int4*>(scol + q0 + j);
-            const float4 v4 = *reinterpret_cast<const float4*>(sval + q0 + j);
+            const int4 c4 = scol4[(j / 4) * 32 + lane];    // my entries q0 + j .. q0 + j + 3
+            const float4 v4 = sval4[(j / 4) * 32 + lane];
             // ld.global.cg: the gathers are served by L2; caching them in L1
             // only evicts lines other warps are waiting on.
             xv[j] = spmv_gather<kG>(x, hs, A, c4.x); xv[j + 1] = spmv_gather<kG>(x, hs, A, c4.y);
             xv[j + 2] = spmv_gather<kG>(x, hs, A, c4.z); xv[j + 3] = spmv_gather<kG>(x, hs, A, c4.w);
             vv[j] = v4.x; vv[j + 1] = v4.y; vv[j + 2] = v4.z; vv[j + 3] = v4.w;
             if constexpr (kLo) {
-                const float4 l4 = *reinterpret_cast<const float4*>(slo + q0 + j);
+                const float4 l4 = slo4[(j / 4) * 32 + lane];
                 ll[j] = l4.x; ll[j + 1] = l4.y; ll[j + 2] = l4.z; ll[j + 3] = l4.w;
             }
         }
