@@ -406,10 +406,12 @@ PRAMAAN_API int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* by
                                  double* bytes_primal);
 /* Gather modes (option gather_cache) of the dual product's operand A and the
  * primal product's operand A^T: hot gather slots (entries of x kept in shared
- * memory) and whether the gathers are cached in L1 (1) or not (0).  Any
- * pointer may be NULL. */
+ * memory), whether the gathers are cached in L1 (1) or not (0), and the
+ * resident blocks per SM the launch autotuner chose (0: the default grid).
+ * Any pointer may be NULL. */
 PRAMAAN_API int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual,
-                                int32_t* slots_primal, int32_t* l1_dual, int32_t* l1_primal);
+                                int32_t* slots_primal, int32_t* l1_dual, int32_t* l1_primal,
+                                int32_t* blocks_dual, int32_t* blocks_primal);
 
 #ifdef __cplusplus
 }

@@ -118,7 +118,7 @@ SIGNATURES = [
     ("pramaan_session_kernel_times", C.c_int,
      [P, C.POINTER(f64), C.POINTER(f64), C.POINTER(i64), i32]),
     ("pramaan_session_kernel_bytes", C.c_int, [P, C.POINTER(f64), C.POINTER(f64)]),
-    ("pramaan_session_gather_info", C.c_int, [P, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]),
+    ("pramaan_session_gather_info", C.c_int, [P] + [C.POINTER(i32)] * 6),
 ]
 
 _lib: C.CDLL | None = None

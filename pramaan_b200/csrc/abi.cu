@@ -391,13 +391,16 @@ int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual, do
 }
 
 int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual, int32_t* slots_primal,
-                                int32_t* l1_dual, int32_t* l1_primal) {
+                                int32_t* l1_dual, int32_t* l1_primal, int32_t* blocks_dual,
+                                int32_t* blocks_primal) {
     return guarded([&] {
         if (!s) throw InvalidArgument("session is NULL");
         if (slots_dual) *slots_dual = s->eng->hot_slots_dual();
         if (slots_primal) *slots_primal = s->eng->hot_slots_primal();
         if (l1_dual) *l1_dual = s->eng->gather_l1_dual();
         if (l1_primal) *l1_primal = s->eng->gather_l1_primal();
+        if (blocks_dual) *blocks_dual = s->eng->blocks_dual();
+        if (blocks_primal) *blocks_primal = s->eng->blocks_primal();
     });
 }
 

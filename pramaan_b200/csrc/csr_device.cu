@@ -518,7 +518,7 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int g
             const CsrView v = A.view(false);
             Launch::launch(v, xs.get(), epi, status, st, dev);   // warm-up
             PB_CUDA_CHECK(cudaEventRecord(e0, st));
-            for (int r = 0; r < 3; ++r) Launch::launch(v, xs.get(), epi, status, st, dev);
+            for (int r = 0; r < 5; ++r) Launch::launch(v, xs.get(), epi, status, st, dev);
             PB_CUDA_CHECK(cudaEventRecord(e1, st));
             PB_CUDA_CHECK(cudaEventSynchronize(e1));
             float ms = 0.f;

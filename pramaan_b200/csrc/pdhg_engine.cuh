@@ -54,6 +54,8 @@ public:
     int hot_slots_primal() const { return AT_.hot; }
     int gather_l1_dual() const { return A_.gather_l1; }
     int gather_l1_primal() const { return AT_.gather_l1; }
+    int blocks_dual() const { return A_.tuned_blocks_per_sm; }
+    int blocks_primal() const { return AT_.tuned_blocks_per_sm; }
     void synchronize();
 
     // ---- adaptive mode (pdhg_adaptive.cu) ----

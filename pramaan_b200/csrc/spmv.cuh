@@ -350,14 +350,18 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
         const int s0 = int(fl[0] & 1u);                                 // tile's first entry starts a row
 
         // ---- row ids: first_row + #starts in (0, q] ----
-        int incl = __popc(my);
+        // Each lane's start count (0..16) in five bit-planes: one ballot per
+        // plane gives the exclusive prefix and the total without shuffles.
+        const int cnt = __popc(my);
+        int excl = 0, starts_total = 0;
+        const unsigned below = (1u << lane) - 1u;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += v;
+        for (int b = 0; b < 5; ++b) {
+            const unsigned plane = __ballot_sync(0xffffffffu, (cnt >> b) & 1);
+            excl += __popc(plane & below) << b;
+            starts_total += __popc(plane) << b;
         }
-        const int starts_total = __shfl_sync(0xffffffffu, incl, 31);
-        const int row0 = meta.x + (incl - __popc(my)) + int(my & 1u) - s0;
+        const int row0 = meta.x + excl + int(my & 1u) - s0;
         const bool head_before = (my & 1u) == 0;   // my first row began before my first entry
 
         // Rows finished in this tile are meta.x .. meta.x + ends_total - 1.  When
@@ -395,13 +399,16 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
         }
 
         // ---- segmented warp scan of (row end seen, open partial) ----
-        int f = nemit > 0 ? 1 : 0;
+        // Before the step of distance d, lane i's partial covers lanes
+        // (i-d, i]; it takes lane i-d's only when no lane in that window
+        // ended a row, read from one ballot of the row ends.
+        const unsigned ended = __ballot_sync(0xffffffffu, nemit > 0) & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));
         AccT v = acc;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const int fo = __shfl_up_sync(0xffffffffu, f, d);
             const AccT vo = __shfl_up_sync(0xffffffffu, v, d);
-            if (lane >= d) { if (!f) v += vo; f |= fo; }
+            const int lo = lane - d + 1 > 0 ? lane - d + 1 : 0;
+            if (lane >= d && (ended >> lo) == 0u) v += vo;
         }
         AccT carry_in = __shfl_up_sync(0xffffffffu, v, 1);   // partial of the row open at q0
         if (lane == 0) carry_in = AccT(0);

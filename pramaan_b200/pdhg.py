@@ -379,11 +379,12 @@ class Session:
     def gather_info(self) -> dict:
         """Gather modes of the dual product's operand A and the primal
         product's operand A^T: hot gather slots (0: no shared-memory copy) and
-        whether the gathers are cached in L1."""
-        v = [C.c_int32() for _ in range(4)]
+        whether the gathers are cached in L1, and the autotuned resident
+        blocks per SM (0: default grid)."""
+        v = [C.c_int32() for _ in range(6)]
         L.check(L.lib().pramaan_session_gather_info(self._h, *(C.byref(q) for q in v)))
-        return {"A": {"hot_slots": v[0].value, "l1": bool(v[2].value)},
-                "AT": {"hot_slots": v[1].value, "l1": bool(v[3].value)}}
+        return {"A": {"hot_slots": v[0].value, "l1": bool(v[2].value), "blocks_per_sm": v[4].value},
+                "AT": {"hot_slots": v[1].value, "l1": bool(v[3].value), "blocks_per_sm": v[5].value}}
 
     def gather_slots(self) -> tuple[int, int]:
         """Hot gather slots of A and A^T."""

@@ -86,8 +86,9 @@ def test_l1_cached_gathers_identical_to_l2_gathers(banded_mid):
             x, y = s.iterates()
         runs[cache] = (info, res, x, y)
     forced, auto, off = runs[1], runs[0], runs[-1]
-    assert forced[0]["A"] == {"hot_slots": 0, "l1": True} and forced[0]["AT"] == {"hot_slots": 0, "l1": True}
-    assert off[0]["A"] == {"hot_slots": 0, "l1": False} and off[0]["AT"] == {"hot_slots": 0, "l1": False}
+    for op in ("A", "AT"):
+        assert (forced[0][op]["hot_slots"], forced[0][op]["l1"]) == (0, True)
+        assert (off[0][op]["hot_slots"], off[0][op]["l1"]) == (0, False)
     assert auto[0]["A"]["hot_slots"] == 0 and auto[0]["AT"]["hot_slots"] == 0
     for run in (forced, auto):
         assert np.array_equal(run[2], off[2]) and np.array_equal(run[3], off[3])
