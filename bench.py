@@ -358,6 +358,7 @@ def learned_stream_section(args, device):
     for mode in ("cold", "hint", "learned"):
         prev = None
         its, t, ok, cert, choices = 0, 0.0, 0, 0, {}
+        phases = {"predict_s": 0.0, "certify_s": 0.0, "solve_s": 0.0, "fallback_s": 0.0, "fallbacks": 0}
         for w in range(W):
             batch = windows[w]
             hints = None if prev is None else _hints_for(batch, prev)
@@ -370,6 +371,8 @@ def learned_stream_section(args, device):
                 res, info = warm_solve_batch(batch, net, o, hints=hints)
                 for c in info.choices:
                     choices[c] = choices.get(c, 0) + 1
+                for k in phases:
+                    phases[k] += getattr(info, k)
             t += time.perf_counter() - t0
             its += sum(r.iterations for r in res)
             ok += sum(r.status == SolveStatus.kOptimal for r in res)
@@ -378,6 +381,7 @@ def learned_stream_section(args, device):
         out[mode] = {"lps_per_s": S * W / t, "seconds": t, "iterations": its, "optimal": ok, "certified": cert}
         if choices:
             out[mode]["starts"] = choices
+            out[mode]["phases"] = phases
     for mode in ("hint", "learned"):
         out[mode]["iterations_vs_cold"] = out[mode]["iterations"] / out["cold"]["iterations"]
         out[mode]["speedup_vs_cold"] = out[mode]["lps_per_s"] / out["cold"]["lps_per_s"]
