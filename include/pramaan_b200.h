@@ -404,6 +404,12 @@ PRAMAAN_API int pramaan_session_kernel_times(pramaan_pdhg_session* s, double* ms
  * notes in the library documentation). */
 PRAMAAN_API int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* bytes_dual,
                                  double* bytes_primal);
+/* Frees the device memory the library keeps for reuse on device `device`
+ * (-1: every device).  Solves allocate their operands and temporaries from a
+ * per-device cache (at most 32 GB kept per device) so that repeated solves
+ * skip cudaMalloc / cudaFree; this returns that memory to the driver. */
+PRAMAAN_API int pramaan_release_cached_memory(int32_t device);
+
 /* Gather modes (option gather_cache) of the dual product's operand A and the
  * primal product's operand A^T: hot gather slots (entries of x kept in shared
  * memory), whether the gathers are cached in L1 (1) or not (0), and the

@@ -17,6 +17,7 @@ from .pdhg import (  # noqa: F401
     launch_pdhg_iteration,
     launch_spmv,
     launch_spmv_t,
+    release_cached_memory,
     solve_batch,
 )
 from ._lib import LIB_PATH, PramaanError, lib  # noqa: F401

@@ -119,6 +119,7 @@ SIGNATURES = [
      [P, C.POINTER(f64), C.POINTER(f64), C.POINTER(i64), i32]),
     ("pramaan_session_kernel_bytes", C.c_int, [P, C.POINTER(f64), C.POINTER(f64)]),
     ("pramaan_session_gather_info", C.c_int, [P] + [C.POINTER(i32)] * 6),
+    ("pramaan_release_cached_memory", C.c_int, [i32]),
 ]
 
 _lib: C.CDLL | None = None

@@ -404,6 +404,13 @@ int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual, in
     });
 }
 
+int pramaan_release_cached_memory(int32_t device) {
+    return guarded([&] {
+        if (device < -1) throw InvalidArgument("device must be -1 or a device ordinal");
+        device_cache_release(device);
+    });
+}
+
 // ---- precision ladder ----------------------------------------------------
 
 void pramaan_ladder_default_options(pramaan_ladder_options* opt) {

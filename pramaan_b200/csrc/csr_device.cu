@@ -3,6 +3,10 @@
 #include "csr_device.cuh"
 #include "epilogues.cuh"
 
+#include <map>
+#include <mutex>
+#include <unordered_map>
+
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -235,6 +239,114 @@ __global__ void slot_scatter_kernel(const int* __restrict__ ids, int H, int* __r
 }
 
 }  // namespace
+
+namespace {
+
+constexpr size_t kDeviceCacheCap = size_t(32) << 30;   // bytes kept per device
+constexpr int kMaxDevices = 64;
+
+struct DeviceCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks[kMaxDevices];   // by size
+    size_t cached[kMaxDevices] = {};
+    struct Block { size_t bytes; int dev; };
+    std::unordered_map<void*, Block> live;                    // handed out
+};
+
+DeviceCache& device_cache() {
+    static DeviceCache* c = new DeviceCache;   // kept to process exit
+    return *c;
+}
+
+size_t cache_round(size_t b) {
+    const size_t g = b < (size_t(1) << 20) ? 256 : (size_t(2) << 20);
+    return (b + g - 1) / g * g;
+}
+
+}  // namespace
+
+void* device_cache_alloc(size_t bytes) {
+    int dev = 0;
+    PB_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("device_cache_alloc: device ordinal out of range");
+    const size_t want = cache_round(bytes);
+    DeviceCache& c = device_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto& fb = c.free_blocks[dev];
+        auto it = fb.lower_bound(want);
+        if (it != fb.end() && it->first <= 2 * want) {
+            void* p = it->second;
+            const size_t sz = it->first;
+            fb.erase(it);
+            c.cached[dev] -= sz;
+            c.live[p] = {sz, dev};
+            return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaErrorMemoryAllocation) {
+        (void)cudaGetLastError();
+        device_cache_release(dev);
+        e = cudaMalloc(&p, want);
+    }
+    PB_CUDA_CHECK(e);
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.live[p] = {want, dev};
+    return p;
+}
+
+void device_cache_free(void* p) noexcept {
+    DeviceCache& c = device_cache();
+    DeviceCache::Block b{0, 0};
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.live.find(p);
+        if (it == c.live.end()) return;
+        b = it->second;
+        c.live.erase(it);
+    }
+    int cur = -1;
+    (void)cudaGetDevice(&cur);
+    if (cur != b.dev) (void)cudaSetDevice(b.dev);
+    // cudaFree waits for the device; a cached block must not be reused while
+    // work issued before its release may still read or write it
+    const cudaError_t e = cudaDeviceSynchronize();
+    bool keep = e == cudaSuccess;
+    if (keep) {
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.cached[b.dev] + b.bytes <= kDeviceCacheCap) {
+            c.free_blocks[b.dev].emplace(b.bytes, p);
+            c.cached[b.dev] += b.bytes;
+        } else {
+            keep = false;
+        }
+    }
+    if (!keep) (void)cudaFree(p);
+    if (cur >= 0 && cur != b.dev) (void)cudaSetDevice(cur);
+}
+
+void device_cache_release(int dev) {
+    DeviceCache& c = device_cache();
+    std::vector<std::pair<int, void*>> out;
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        for (int d = 0; d < kMaxDevices; ++d) {
+            if (dev >= 0 && d != dev) continue;
+            for (auto& kv : c.free_blocks[d]) out.emplace_back(d, kv.second);
+            c.free_blocks[d].clear();
+            c.cached[d] = 0;
+        }
+    }
+    int cur = -1;
+    (void)cudaGetDevice(&cur);
+    for (auto& [d, p] : out) {
+        if (d != cur) (void)cudaSetDevice(d);
+        (void)cudaFree(p);
+        if (d != cur && cur >= 0) (void)cudaSetDevice(cur);
+    }
+}
 
 void CsrDevice::select_hot(const int* target_rp, int num_targets, int dev, cudaStream_t st) {
     hot = 0;

@@ -40,8 +40,21 @@
 namespace pb {
 
 // ---------------------------------------------------------------------------
-// RAII device buffer
+// Device allocations go through a process-wide cache (csr_device.cu): a
+// solve allocates and frees several GB of operands and temporaries, and
+// cudaMalloc / cudaFree of that much memory cost more per call than the
+// transfers.  A freed block first waits for the device (cudaFree's
+// synchronisation, which callers may rely on), then is kept for reuse by a
+// later allocation of up to its size on the same device (best fit, at most
+// twice the request); kDeviceCacheCap bytes at most are kept per device, and
+// a failed cudaMalloc releases the cache and retries.
 // ---------------------------------------------------------------------------
+void* device_cache_alloc(size_t bytes);
+void device_cache_free(void* p) noexcept;
+// Frees the cached blocks of device `dev` (-1: every device).
+void device_cache_release(int dev);
+
+// RAII device buffer
 template <typename T>
 class DevBuf {
 public:
@@ -58,11 +71,11 @@ public:
     void alloc(size_t n) {
         reset();
         if (n == 0) return;
-        PB_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+        p_ = static_cast<T*>(device_cache_alloc(n * sizeof(T)));
         n_ = n;
     }
     void reset() {
-        if (p_) cudaFree(p_);
+        if (p_) device_cache_free(p_);
         p_ = nullptr;
         n_ = 0;
     }

@@ -317,6 +317,12 @@ def launch_pdhg_iteration(x: np.ndarray, y: np.ndarray, gradient, Ax_bar, b,  # 
         _ptr(x), _ptr(y), _ptr(g), _ptr(ax), _ptr(bb), len(x), len(y), float(tau), float(sigma)))
 
 
+def release_cached_memory(device: int = -1) -> None:
+    """Returns the device memory the library keeps for reuse to the driver
+    (pramaan_release_cached_memory; -1: every device)."""
+    L.check(L.lib().pramaan_release_cached_memory(int(device)))
+
+
 class Session:
     """Device-resident solver state (pramaan_session_* entry points)."""
 
