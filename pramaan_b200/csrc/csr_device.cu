@@ -5,6 +5,7 @@
 
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <unordered_map>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -605,11 +606,37 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st) {
 // Launch autotuner: picks the resident blocks per SM and the gather mode for
 // one operand by timing the SpMV (store-only epilogue into scratch, so no
 // iterate changes) for every candidate, and records the fastest in the operand.
+namespace {
+
+// Tuned launch shapes by operand signature, so repeated solves of the same
+// operand (the same LP, or LPs of one generator and size) skip the timing.
+struct TuneKey {
+    int dev, rows, cols, nnz, tiles, cross, empty, hot, gather_cache;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(dev, rows, cols, nnz, tiles, cross, empty, hot, gather_cache) <
+               std::tie(o.dev, o.rows, o.cols, o.nnz, o.tiles, o.cross, o.empty, o.hot, o.gather_cache);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tuned;   // -> {blocks per SM, gather_l1}
+
+}  // namespace
+
 void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache) {
     using Epi = EpiStore<float, float>;
     using Launch = SpmvLauncher<Epi, float, float, false>;
     A.gather_l1 = (gather_cache > 0 && A.hot == 0) ? 1 : 0;
     if (A.num_tiles < 4 * device_sm_count(dev)) return;   // small operands: default grid
+    const TuneKey key{dev, A.rows, A.cols, A.nnz, A.num_tiles, A.num_cross, A.num_empty, A.hot, gather_cache};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        const auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            A.tuned_blocks_per_sm = it->second.first;
+            A.gather_l1 = it->second.second;
+            return;
+        }
+    }
     const int occ = A.hot > 0 ? Launch::hot_blocks_per_sm(dev) : Launch::blocks_per_sm(dev);
     // L1-cached gathers are a candidate for operands without hot slots; the
     // L2 mode is timed first and kept unless the other is 2 % faster.
@@ -642,6 +669,8 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int g
     cudaEventDestroy(e1);
     A.tuned_blocks_per_sm = best_bps;
     A.gather_l1 = best_mode;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = {best_bps, best_mode};
 }
 
 

@@ -168,7 +168,9 @@ void select_hot_pair(CsrDevice& A, CsrDevice& AT, int dev, cudaStream_t st);
 // ---------------------------------------------------------------------------
 int device_sm_count(int dev);
 
-// Launch autotuner: times the store-only product of `A` at 1-4 resident
+// Launch autotuner (results remembered per device and operand signature:
+// shape, crossing and empty rows, hot slots, option): times the store-only
+// product of `A` at 1-4 resident
 // blocks per SM and, for an operand without hot slots, with L2 and with
 // L1-cached gathers, and records the fastest in A.tuned_blocks_per_sm and
 // A.gather_l1 (operands with fewer than 4 tiles per SM keep the default grid
