@@ -276,7 +276,7 @@ def rolling_horizon_section(args, device, dist=None):
     tol = 1e-6
     world = dist.get_world_size() if dist else 1
     rank = dist.get_rank() if dist else 0
-    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
+    o = PdhgOptions(tolerance=tol, max_iterations=400000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)
     models = rolling_horizon_batch(args.rh_count * world, seed=args.seed)
     mine = shard_plan([m.nnz() for m in models], world)[rank]
@@ -337,7 +337,7 @@ def learned_stream_section(args, device):
     net = WarmStartNet(device=device, seed=0)
     net.load(DEFAULT_OUT)
     tol = 1e-6
-    o = PdhgOptions(tolerance=tol, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
+    o = PdhgOptions(tolerance=tol, max_iterations=400000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)
     S, W = args.stream_count, args.stream_windows
     ms, _ = stream_windows(range(700000 + args.seed, 700000 + args.seed + S), W, tuple(rec["T"]), tuple(rec["P"]))

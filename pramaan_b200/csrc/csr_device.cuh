@@ -298,7 +298,7 @@ struct SpmvLauncher {
     // Grid for one launch: A.blocks_per_sm (autotuned) or the default target,
     // never more than fit, never more blocks than tile groups.
     // For an operand with hot slots the tuned value applies to the FP32 hot
-    // kernel (the one the tuner times); the kHot 2 kernels use the default.
+    // kernel (the one the tuner times); the kGatherHotIdx kernels use the default.
     static int grid_for(const CsrView& A, int dev) {
         const bool mapped = A.row_map != nullptr;
         const bool hot = A.hot > 0;
