@@ -147,7 +147,7 @@ constexpr float kHalpernReflection = 1.0f;
 
 __device__ __forceinline__ float halpern_weight(const int* iter_base, int offset, const int* restart_iter,
                                                 const int* lp, int i) {
-    const long long k = (long long)(*iter_base) + offset - restart_iter[lp[i]];
+    const long long k = (long long)(*iter_base) + offset - restart_iter[lp ? lp[i] : 0];   // lp null: one LP
     return k <= 0 ? 0.5f : float(double(k + 1) / double(k + 2));
 }
 
@@ -168,7 +168,7 @@ struct EpiPrimalHalpern {
     __device__ void init(State&) const {}
     __device__ void prefetch(int j) const {
         prefetch_l2(tau + j); prefetch_l2(c + j); prefetch_l2(l_x + j); prefetch_l2(u_x + j);
-        prefetch_l2(x + j); prefetch_l2(lp + j);
+        prefetch_l2(x + j); if (lp) prefetch_l2(lp + j);
     }
     __device__ void apply(State&, int j, float aty) const {
         const float x_prev = x[j];
@@ -209,7 +209,7 @@ struct EpiDualHalpern {
     __device__ void init(State&) const {}
     __device__ void prefetch(int i) const {
         prefetch_l2(sigma + i); prefetch_l2(r_lo + i); prefetch_l2(r_hi + i); prefetch_l2(y_m + i);
-        prefetch_l2(e + i); prefetch_l2(lp + i);
+        prefetch_l2(e + i); if (lp) prefetch_l2(lp + i);
     }
     __device__ void apply(State&, int i, float ad) const {
         const float s = sigma[i];

@@ -731,12 +731,15 @@ void AdaptiveBatch::iterate_once(int j, int k) {
         // the anchor is the restart point, which the fold made the master: 0 in correction space
         const float* ax = nullptr;
         const float* ay = nullptr;
-        EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(), ax, lp_col_.get(),
+        // a batch of one LP reads its restart counter without per-row LP indices
+        const int* lpc = K_ == 1 ? nullptr : lp_col_.get();
+        const int* lpr = K_ == 1 ? nullptr : lp_row_.get();
+        EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(), ax, lpc,
                             restart_iter_.get(), iter_base_.get(), j, fc};
         SpmvLauncher<EpiPrimalHalpern, float, float, false>::launch(AT_.view(false), y_.get(), ep, status_.get(), st_,
                                                                    dev_);
         if (m_ > 0) {
-            EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), ay, lp_row_.get(),
+            EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), ay, lpr,
                               restart_iter_.get(), iter_base_.get(), j, fr};
             SpmvLauncher<EpiDualHalpern, float, float, false>::launch(A_.view(false), xbar_.get(), ed, status_.get(),
                                                                      st_, dev_);
@@ -769,9 +772,11 @@ void AdaptiveBatch::launch_interval(int k) {
         gsync_.alloc(2);
         PB_CUDA_CHECK(cudaMemsetAsync(gsync_.get(), 0, gsync_.bytes(), st_));
     }
-    EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(), nullptr, lp_col_.get(),
+    const int* lpc = K_ == 1 ? nullptr : lp_col_.get();   // one LP: no per-row LP indices
+    const int* lpr = K_ == 1 ? nullptr : lp_row_.get();
+    EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(), nullptr, lpc,
                         restart_iter_.get(), iter_base_.get(), 0, nullptr};
-    EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), nullptr, lp_row_.get(),
+    EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), nullptr, lpr,
                       restart_iter_.get(), iter_base_.get(), 0, nullptr};
     const CsrView va = A_.view(false), vat = AT_.view(false);
     GridSync gs{gsync_.get(), gsync_.get() + 1, unsigned(grid)};
