@@ -205,9 +205,14 @@ def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    import torch
+
     from pramaan_b200.generators import zipf_lp
 
-    model = zipf_lp(args.m, args.n, cap=args.cap, seed=args.seed, device="cpu")
+    # the same instance as the GPU arm: torch's CPU and CUDA generators draw
+    # different streams, so generate where that arm does when a GPU is present
+    gen_dev = "cuda:0" if torch.cuda.is_available() else "cpu"
+    model = zipf_lp(args.m, args.n, cap=args.cap, seed=args.seed, device=gen_dev)
     import oracle
     from oracle import ptr
 
