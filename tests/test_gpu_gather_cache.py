@@ -104,3 +104,38 @@ def test_halpern_with_hot_slots_and_l1_gathers_identical(zipf_mid):
     a, b = out[1], out[-1]
     assert a.iterations == b.iterations
     assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+
+
+def _with_empty_rows_and_columns(md):
+    """The LP with the entries of every 7th column and every 11th row removed,
+    so both operands compact empty rows away (row maps) while A^T keeps its
+    hot targets."""
+    from pramaan_b200.pdhg import ModelIR
+
+    rows = np.repeat(np.arange(md.numRows()), np.diff(md.row_ptr))
+    keep = (md.col_idx % 7 != 0) & (rows % 11 != 0)
+    rp = np.zeros(md.numRows() + 1, np.int64)
+    np.cumsum(np.bincount(rows[keep], minlength=md.numRows()), out=rp[1:])
+    return ModelIR(md.obj_coeffs, rp, md.col_idx[keep], md.values[keep], md.row_lower, md.row_upper,
+                   md.var_lower, md.var_upper, md.obj_sense, md.obj_offset)
+
+
+def test_hot_slots_with_row_maps_identical(zipf_mid):
+    md = _with_empty_rows_and_columns(zipf_mid)
+    runs = {}
+    for cache in (0, 1, -1):
+        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+                        gather_cache=cache)
+        with Session(md, o) as s:
+            info = s.gather_info()
+            s.iterate(40)
+            res = s.residuals()
+            x, y = s.iterates()
+        runs[cache] = (info, res, x, y)
+    assert runs[0][0]["AT"]["hot_slots"] > 1000 and runs[-1][0]["AT"]["hot_slots"] == 0
+    assert runs[1][0]["A"]["l1"]
+    for cache in (0, 1):
+        assert np.array_equal(runs[cache][2], runs[-1][2]) and np.array_equal(runs[cache][3], runs[-1][3])
+        assert runs[cache][1] == runs[-1][1]
+    # the emptied columns keep their clamped start; the emptied rows move only with their bounds
+    assert np.isfinite(runs[0][2]).all()
