@@ -67,6 +67,12 @@ __global__ void diag_step_kernel(const int* __restrict__ row_ptr, const float* _
     }
 }
 
+// FP32 -> FP64 copy of an iterate (the answer's x and y).
+__global__ void widen_kernel(const float* __restrict__ v, int n, double* __restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = static_cast<double>(v[i]);
+}
+
 __global__ void init_primal_kernel(const float* __restrict__ lx, const float* __restrict__ ux,
                                    int n, float* __restrict__ x, float* __restrict__ xbar) {
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
@@ -485,26 +491,38 @@ void PdhgEngine::solve(const pramaan_lp& lp, pramaan_solve_result* res) {
         if (nonfinite && res->status == PRAMAAN_STATUS_OPTIMAL)
             res->status = PRAMAAN_STATUS_NUMERICAL_FAILURE;
     }
-    std::vector<double> hx(static_cast<size_t>(n_)), hy(static_cast<size_t>(m_));
+    // x and y in FP64 straight into the caller's arrays (x into a host copy
+    // when the caller passed none, for the objective); FP32 iterates are
+    // widened on the device, so one copy crosses PCIe
+    std::vector<double> hx_own;
+    double* hx = res->x;
+    if (!hx && n_ > 0) {
+        hx_own.resize(static_cast<size_t>(n_));
+        hx = hx_own.data();
+    }
+    double* hy = m_ > 0 ? res->y : nullptr;
     if (master_out_) {
         // the FP64 master iterate is the answer
-        if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(hx.data(), x64_.get(), size_t(n_) * 8, cudaMemcpyDeviceToHost, st_));
-        if (m_) PB_CUDA_CHECK(cudaMemcpyAsync(hy.data(), y64_.get(), size_t(m_) * 8, cudaMemcpyDeviceToHost, st_));
+        if (n_) PB_CUDA_CHECK(cudaMemcpyAsync(hx, x64_.get(), size_t(n_) * 8, cudaMemcpyDeviceToHost, st_));
+        if (hy) PB_CUDA_CHECK(cudaMemcpyAsync(hy, y64_.get(), size_t(m_) * 8, cudaMemcpyDeviceToHost, st_));
         synchronize();
     } else {
-        std::vector<float> fx(static_cast<size_t>(n_)), fy(static_cast<size_t>(m_));
-        get_iterates(fx.data(), fy.data());
-        for (int j = 0; j < n_; ++j) hx[j] = static_cast<double>(fx[j]);
-        for (int i = 0; i < m_; ++i) hy[i] = static_cast<double>(fy[i]);
+        DevBuf<double> xd(static_cast<size_t>(n_)), yd(static_cast<size_t>(hy ? m_ : 0));
+        if (n_) {
+            widen_kernel<<<grid_1d(n_), kThreads, 0, st_>>>(x_.get(), n_, xd.get());
+            PB_CUDA_CHECK(cudaGetLastError());
+            PB_CUDA_CHECK(cudaMemcpyAsync(hx, xd.get(), size_t(n_) * 8, cudaMemcpyDeviceToHost, st_));
+        }
+        if (hy) {
+            widen_kernel<<<grid_1d(m_), kThreads, 0, st_>>>(y_.get(), m_, yd.get());
+            PB_CUDA_CHECK(cudaGetLastError());
+            PB_CUDA_CHECK(cudaMemcpyAsync(hy, yd.get(), size_t(m_) * 8, cudaMemcpyDeviceToHost, st_));
+        }
+        synchronize();
     }
     double obj = lp.obj_offset;
-    for (int j = 0; j < n_; ++j) {
-        if (res->x) res->x[j] = hx[j];
-        obj += lp.obj_coeffs[j] * hx[j];
-    }
+    for (int j = 0; j < n_; ++j) obj += lp.obj_coeffs[j] * hx[j];
     res->objective_value = obj;
-    if (res->y)
-        for (int i = 0; i < m_; ++i) res->y[i] = hy[i];
     if (res->row_activity && m_ > 0) {
         DevBuf<double> act{size_t(m_)};
         EpiStore<double, double> epi{act.get()};
