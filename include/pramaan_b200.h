@@ -396,8 +396,10 @@ PRAMAAN_API int pramaan_session_residuals(pramaan_pdhg_session* s, double* prima
 PRAMAAN_API int pramaan_session_get_iterates(pramaan_pdhg_session* s, float* x, float* y);
 /* The cudaStream_t the session launches on. */
 PRAMAAN_API void* pramaan_session_stream(pramaan_pdhg_session* s);
-/* Accumulated CUDA-event time (ms) and launch count of the two product
- * kernels since the last reset (profile_kernels must be set; synchronises). */
+/* Accumulated CUDA-event time (ms) of the two products and the number of
+ * kernels they launched since the last reset (a product is its main kernel
+ * plus, when rows cross tiles, their completion kernel; profile_kernels must
+ * be set; synchronises). */
 PRAMAAN_API int pramaan_session_kernel_times(pramaan_pdhg_session* s, double* ms_dual, double* ms_primal,
                                  int64_t* launches, int32_t reset);
 /* Algorithmic bytes of one launch of each product kernel (see the layout

@@ -317,7 +317,10 @@ void PdhgEngine::drain_events() {
         float ms = 0.f;
         PB_CUDA_CHECK(cudaEventElapsedTime(&ms, ev_pool_[i].a, ev_pool_[i].b));
         if (ev_pool_[i].kind == 0) ms_dual_ += ms; else ms_primal_ += ms;
-        ++launches_;
+        // kernels of one product: the main kernel and, when rows cross tiles, their completion
+        launches_ += ev_pool_[i].kind == 0
+                         ? SpmvLauncher<EpiDualRef, float, float, false>::launches(A_.view(false))
+                         : SpmvLauncher<EpiPrimalRef, float, float, false>::launches(AT_.view(false));
     }
     ev_used_ = 0;
 }
