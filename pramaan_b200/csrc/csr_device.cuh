@@ -181,12 +181,14 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int g
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
 // Hot-slot kernel: one block per SM of kSpmvHotWarps warps (aliased staging,
-// ~92 KB) plus the 64 KB FP32 hot copy, which keeps the 164 KB shared-memory
+// ~109 KB) plus the 48 KB FP32 hot copy, which keeps the 164 KB shared-memory
 // carve-out and so ~92 KB of L1 for the outstanding cold gathers.  Measured on
-// the 2,000,000 x 5,000,000 Zipf LP: 8 warps 0.548 ms, 11 warps 0.459 ms, 14
-// warps with an 8 K-slot copy 0.459 ms, no hot slots 0.505 ms per A^T y.
-constexpr int kSpmvHotWarps = 11;
-constexpr int kSpmvHotCap = 16384;            // most hot slots
+// the 2,000,000 x 5,000,000 Zipf LP (A^T y per launch): 11 warps with a 16 K-slot
+// copy 0.390 ms, 13 warps with 12 K slots 0.386 ms, 14 warps with 8 K slots
+// 0.412 ms (earlier kernel generation: 8 warps / 16 K 0.548 ms, 11 / 16 K 0.459
+// ms, no hot slots 0.505 ms).
+constexpr int kSpmvHotWarps = 13;
+constexpr int kSpmvHotCap = 12288;            // most hot slots (48 KB FP32 copy)
 constexpr int kSpmvHotMinUses = 2;            // gathers per slot per resident block
 constexpr double kSpmvHotMinShare = 0.15;     // share of the non-zeros the slots must take
 
