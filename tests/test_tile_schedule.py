@@ -307,3 +307,71 @@ def test_noalloc_schedule_random_structures(mode):
             expect = int(prod[rp[r]:rp[r + 1]].sum())
             assert r in y, (trial, r)          # every row is written, empty rows with 0
             assert y[r] == expect, (trial, r)
+
+
+# ---- integer transformations inside the tile loop ---------------------------
+# The kernel computes two warp-level integer results with ballots instead of
+# shuffles, and reads its entries through a lane-interleaved record layout.
+# These restate both forms and check that they agree exactly.
+
+IPT = 16
+
+
+def tile_slot(q):
+    """Slot of tile-local entry q in a record (spmv.cuh tile_slot): chunk k of
+    lane l (entries 16l + 4k .. 16l + 4k + 3) at chunk index k*32 + l."""
+    return (((q % IPT) // 4) * 32 + q // IPT) * 4 + (q % 4)
+
+
+def test_tile_slot_is_a_permutation_with_contiguous_warp_chunks():
+    slots = [tile_slot(q) for q in range(TILE)]
+    assert sorted(slots) == list(range(TILE))
+    for k in range(IPT // 4):                      # chunk read k of the warp
+        starts = [tile_slot(16 * lane + 4 * k) for lane in range(32)]
+        assert starts == list(range(k * 128, k * 128 + 128, 4))   # 512 contiguous bytes
+        for lane in range(32):                     # each chunk holds 4 consecutive entries
+            assert [tile_slot(16 * lane + 4 * k + e) for e in range(4)] == list(range(starts[lane], starts[lane] + 4))
+
+
+def test_ballot_prefix_equals_shuffle_scan():
+    """Exclusive prefix and total of per-lane row-start counts (0..16): five
+    bit-plane ballots against the inclusive shuffle scan it replaced."""
+    rng = np.random.default_rng(5)
+    for _ in range(2000):
+        cnt = rng.integers(0, IPT + 1, 32)
+        incl = np.cumsum(cnt)                                  # shuffle scan
+        planes = [sum(1 << l for l in range(32) if (cnt[l] >> b) & 1) for b in range(5)]
+        for lane in range(32):
+            below = (1 << lane) - 1
+            excl = sum(bin(p & below).count("1") << b for b, p in enumerate(planes))
+            assert excl == incl[lane] - cnt[lane]
+        assert sum(bin(p).count("1") << b for b, p in enumerate(planes)) == incl[-1]
+
+
+def test_ballot_row_end_windows_equal_flag_shuffles():
+    """Segmented scan: at distance d, lane i adds lane i-d's partial only when
+    no lane in (i-d, i] ended a row.  The window test on one ballot of the row
+    ends must equal the OR-propagated flags of the shuffle form it replaced,
+    step for step, and so produce the same sums."""
+    rng = np.random.default_rng(6)
+    for _ in range(2000):
+        ended = rng.random(32) < rng.random()
+        acc = rng.integers(-8, 9, 32).astype(np.int64)
+        mask = sum(1 << l for l in range(32) if ended[l])
+        f = ended.astype(np.int64).copy()
+        v_old, v_new = acc.copy(), acc.copy()
+        d = 1
+        while d < 32:
+            fo = np.array([f[i - d] if i >= d else 0 for i in range(32)])
+            vo_old = np.array([v_old[i - d] if i >= d else 0 for i in range(32)])
+            vo_new = np.array([v_new[i - d] if i >= d else 0 for i in range(32)])
+            for i in range(32):
+                if i >= d and not f[i]:
+                    v_old[i] += vo_old[i]
+                lo = max(0, i - d + 1)
+                ble = mask & ((2 << i) - 1 if i < 31 else 0xFFFFFFFF)
+                if i >= d and (ble >> lo) == 0:
+                    v_new[i] += vo_new[i]
+            f = np.array([(f[i] | fo[i]) if i >= d else f[i] for i in range(32)])
+            d <<= 1
+        assert np.array_equal(v_old, v_new)
