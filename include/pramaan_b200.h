@@ -369,9 +369,14 @@ PRAMAAN_API int pramaan_launch_pdhg_iteration(float* h_x, float* h_y, const floa
  * library until exit), which limits nnz to 134,217,728; larger inputs are
  * rejected with PRAMAAN_ERR_INVALID_ARGUMENT.  Every call shares that array:
  * calls on one stream are ordered, calls that overlap on the GPU race.  The
- * first call on a device looks up the array's device address (no allocation).
- * The CSR is not validated; out-of-range column indices are clamped so they
- * never read outside x. */
+ * first call on a device looks up the array's device address and caches it
+ * for that device's primary context; it allocates nothing itself, but under
+ * lazy module loading it is where the library's module, and with it the
+ * array's storage, may be loaded onto the device.  So make one call per device
+ * before capturing a stream or fixing a memory budget.  The CSR must be well
+ * formed (row_ptr nondecreasing, row_ptr[0] = 0, row_ptr[m] = nnz); it is not
+ * validated, but out-of-range column indices are clamped so they never read
+ * outside x, and row_ptr is never read outside [0, m]. */
 PRAMAAN_API int pramaan_spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_idx,
                                      const float* d_values, int32_t m, int32_t n, int32_t nnz,
                                      const float* d_x, float* d_y, void* stream);

@@ -42,7 +42,11 @@ constexpr int kNaRpCap = kNaTile + 8;                // row_ptr slice capacity
 // piece of the row that begins in tile t and continues past it.
 __device__ __align__(256) float g_noalloc_carry[2 * kNoAllocMaxTiles];
 
+// Per device ordinal: the array's device address and the SM count, looked up
+// once with that device current.  The address belongs to the runtime's primary
+// context of the device, the one every call of this entry point uses.
 std::atomic<float*> g_carry_addr[64];
+std::atomic<int> g_sm_count[64];
 std::mutex g_setup_mutex;
 
 // row_ptr read with the padding convention: row m+1 ends at the padded end.
@@ -86,7 +90,12 @@ __global__ void __launch_bounds__(kNaBlock)
         if (in_smem)
             for (int j = tid; j < cnt; j += kNaBlock) s_rp[j] = rp_at(row_ptr, m, nnz_pad, r_lo + j);
         __syncthreads();
-        auto rp = [&](int r) { return in_smem ? s_rp[r - r_lo] : rp_at(row_ptr, m, nnz_pad, r); };
+        // Rows outside the loaded slice (reachable only when row_ptr is not
+        // nondecreasing) are read from global memory, never past s_rp.
+        auto rp = [&](int r) {
+            const int j = r - r_lo;
+            return (in_smem && j >= 0 && j < cnt) ? s_rp[j] : rp_at(row_ptr, m, nnz_pad, r);
+        };
 
         const int k0 = tile_base + tid * kNaIpt, k1 = k0 + kNaIpt;
         float p[kNaIpt];
@@ -177,19 +186,29 @@ __global__ void noalloc_fixup_kernel(const int* __restrict__ row_ptr, int m, int
     }
 }
 
-// Device address of the scratch array for `dev`, looked up once per device
-// (with that device current) and cached.
-float* carry_address(int dev) {
+// Device address of the scratch array for `dev` (and its SM count), looked up
+// once per device with that device current and cached.  With lazy module
+// loading this first lookup is also where the module, and with it the array,
+// may be loaded onto the device.
+float* carry_address(int dev, int* sms) {
     if (dev < 0 || dev >= 64) throw InvalidArgument("device ordinal out of range");
     float* p = g_carry_addr[dev].load(std::memory_order_acquire);
-    if (p) return p;
+    if (p) {
+        *sms = g_sm_count[dev].load(std::memory_order_relaxed);
+        return p;
+    }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     p = g_carry_addr[dev].load(std::memory_order_relaxed);
-    if (p) return p;
-    void* addr = nullptr;
-    PB_CUDA_CHECK(cudaGetSymbolAddress(&addr, g_noalloc_carry));
-    p = static_cast<float*>(addr);
-    g_carry_addr[dev].store(p, std::memory_order_release);
+    if (!p) {
+        int count = 0;
+        PB_CUDA_CHECK(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev));
+        void* addr = nullptr;
+        PB_CUDA_CHECK(cudaGetSymbolAddress(&addr, g_noalloc_carry));
+        p = static_cast<float*>(addr);
+        g_sm_count[dev].store(count, std::memory_order_relaxed);
+        g_carry_addr[dev].store(p, std::memory_order_release);
+    }
+    *sms = g_sm_count[dev].load(std::memory_order_relaxed);
     return p;
 }
 
@@ -211,14 +230,13 @@ void spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_idx, const floa
         throw InvalidArgument("col_idx, values and x must not be NULL (and n > 0) when nnz > 0");
     int dev = 0;
     PB_CUDA_CHECK(cudaGetDevice(&dev));
-    float* carry = carry_address(dev);
+    int sms = 0;
+    float* carry = carry_address(dev, &sms);
     if (nnz == 0) {
         PB_CUDA_CHECK(cudaMemsetAsync(d_y, 0, size_t(m) * sizeof(float), stream));
         return;
     }
     const int nt = (nnz + kNaTile - 1) / kNaTile;
-    int sms = 0;
-    PB_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int grid = nt < 8 * sms ? nt : 8 * sms;
     noalloc_spmv_kernel<<<grid, kNaBlock, 0, stream>>>(d_row_ptr, d_col_idx, d_values, m, n, nnz,
                                                        d_x, d_y, carry);
