@@ -60,14 +60,27 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--rh-count", type=int, default=128,
-                   help="LPs of the batched rolling-horizon section (the published batch is 512)")
+    p.add_argument("--rh-count", type=int, default=512,
+                   help="LPs of the batched rolling-horizon section (the published batch: 512)")
+    p.add_argument("--ladder-m", type=int, default=200_000, help="rows of the precision-ladder LP")
+    p.add_argument("--ladder-n", type=int, default=500_000, help="columns of the precision-ladder LP")
+    p.add_argument("--no-ladder", action="store_true", help="skip the precision-ladder section")
+    p.add_argument("--solver-cap-s", type=float, default=20.0,
+                   help="wall-clock cap of one reference CPU solve at full size (reported as DNF)")
     p.add_argument("--rh-plain", type=int, default=8, help="LPs of that batch also solved one by one")
     p.add_argument("--stream-count", type=int, default=32, help="streams of the learned warm-start section")
-    p.add_argument("--stream-windows", type=int, default=6, help="windows per stream in that section")
+    p.add_argument("--stream-windows", type=int, default=4, help="windows per stream in that section")
+    p.add_argument("--stream-T", type=int, nargs=2, default=(24, 336), help="periods of the stream windows")
+    p.add_argument("--stream-P", type=int, nargs=2, default=(5, 50), help="products of the stream windows")
+    p.add_argument("--probe-iters", type=int, default=64,
+                   help="PDHG iterations from each candidate start before the certificate chooses")
     p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
     p.add_argument("--no-banded", action="store_true", help="skip the banded-LP bandwidth section")
     p.add_argument("--banded-iters", type=int, default=50)
+    p.add_argument("--only", default=None, choices=["banded", "gnn", "small", "rolling", "stream", "ceiling", "ladder", "solvers"],
+                   help="run one section alone on the given sizes and print its JSON (profiling runs)")
+    p.add_argument("--gnn-lps", type=int, default=64, help="rolling-horizon LPs of the network throughput section")
+    p.add_argument("--gnn-reps", type=int, default=5)
     p.add_argument("--gather-cache", type=int, default=0, choices=[0, 1, -1],
                    help="0: hot gather targets in shared memory, L1-cached gathers where faster (the "
                         "default); 1: L1-cached gathers wherever there are no hot slots; -1: plain")
@@ -159,6 +172,25 @@ def ncu_traffic(kernel_tag: str):
             except ValueError:
                 return None
     return None
+
+
+def gather_ceiling(n: int, device: int) -> dict:
+    """The device's random 4-byte gather rate from an n-entry vector (the
+    library's ceiling kernel), L2 (ld.global.cg) and L1-cached."""
+    import ctypes as C
+
+    import torch
+
+    from pramaan_b200 import _lib as L
+
+    x = torch.rand(n, device=f"cuda:{device}", dtype=torch.float32)
+    torch.cuda.synchronize(device)
+    out = {"n": n}
+    for name, cached in (("l2_gathers_per_s", 0), ("l1_cached_gathers_per_s", 1)):
+        r = C.c_double(0.0)
+        L.check(L.lib().pramaan_measure_gather_rate(x.data_ptr(), n, cached, 5, C.byref(r)))
+        out[name] = r.value
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -345,12 +377,15 @@ def learned_stream_section(args, device):
     o = PdhgOptions(tolerance=tol, max_iterations=400000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)
     S, W = args.stream_count, args.stream_windows
-    ms, _ = stream_windows(range(700000 + args.seed, 700000 + args.seed + S), W, tuple(rec["T"]), tuple(rec["P"]))
+    T, P = tuple(args.stream_T), tuple(args.stream_P)
+    ms, _ = stream_windows(range(700000 + args.seed, 700000 + args.seed + S), W, T, P)
     windows = [[ms[s * W + w] for s in range(S)] for w in range(W)]
-    out = {"workload": f"{S} streams x {W} windows (rolling_horizon_stream, T~U{{{rec['T'][0]}..{rec['T'][1]}}}, "
-                       f"P~U{{{rec['P'][0]}..{rec['P'][1]}}}, AR(1) phi 0.9 sigma 0.1), rel KKT {tol:g}; "
-                       "window w of every stream is one batch",
-           "trained_on": {k: rec[k] for k in ("instances_solved", "instances_trained", "epochs")}}
+    out = {"workload": f"{S} streams x {W} windows (rolling_horizon_stream, T~U{{{T[0]}..{T[1]}}}, "
+                       f"P~U{{{P[0]}..{P[1]}}}, AR(1) phi 0.9 sigma 0.1; a seeded sub-sample of the "
+                       f"10,000-window stream), rel KKT {tol:g}; window w of every stream is one batch",
+           "trained_on": {k: rec[k] for k in ("instances_solved", "instances_trained", "epochs", "T", "P")
+                          if k in rec},
+           "probe_iterations": args.probe_iters}
     solve_batch(windows[0][:2], o)                   # warm-up
     # the plain per-LP solver on a sample of the same windows
     from pramaan_b200 import PdhgSolver
@@ -363,7 +398,8 @@ def learned_stream_section(args, device):
     for mode in ("cold", "hint", "learned"):
         prev = None
         its, t, ok, cert, choices = 0, 0.0, 0, 0, {}
-        phases = {"predict_s": 0.0, "certify_s": 0.0, "solve_s": 0.0, "fallback_s": 0.0, "fallbacks": 0}
+        phases = {"predict_s": 0.0, "certify_s": 0.0, "solve_s": 0.0, "fallback_s": 0.0, "fallbacks": 0,
+                  "probe_iterations": 0}
         for w in range(W):
             batch = windows[w]
             hints = None if prev is None else _hints_for(batch, prev)
@@ -373,11 +409,12 @@ def learned_stream_section(args, device):
             elif mode == "hint":
                 res = solve_batch(batch, o, warm=hints)
             else:
-                res, info = warm_solve_batch(batch, net, o, hints=hints)
+                res, info = warm_solve_batch(batch, net, o, hints=hints, probe_iterations=args.probe_iters)
                 for c in info.choices:
                     choices[c] = choices.get(c, 0) + 1
                 for k in phases:
                     phases[k] += getattr(info, k)
+                its += info.probe_iterations      # every candidate's probe counts
             t += time.perf_counter() - t0
             its += sum(r.iterations for r in res)
             ok += sum(r.status == SolveStatus.kOptimal for r in res)
@@ -422,6 +459,111 @@ def small_lp_section(args, device):
     return out
 
 
+def ladder_section(args, device):
+    """The precision-ladder LP (m = 200,000, n = 500,000, 8 non-zeros per
+    column, row and column scales log-uniform in [1e-4, 1e4], feasible by
+    construction): restarted Halpern PDHG with FP64 refinement to 1e-4, then
+    to 1e-8 relative KKT, each answer certified in FP64 on the GPU."""
+    from pramaan_b200 import PdhgOptions, PdhgSolver
+    from pramaan_b200.certificate import certify
+    from pramaan_b200.generators import ill_conditioned_lp
+    from pramaan_b200.pdhg import ALGO_HALPERN
+
+    md = ill_conditioned_lp(args.ladder_m, args.ladder_n, 8, seed=args.seed)
+    out = {"workload": f"ill_conditioned_lp {args.ladder_m} x {args.ladder_n}, 8 nnz/col, scales 10^+-4, "
+                       f"seed {args.seed}", "nnz": int(md.nnz())}
+    PdhgSolver(PdhgOptions(tolerance=1e-2, algorithm=ALGO_HALPERN, check_frequency=64, device=device)).solve(md)
+    for tol in (1e-4, 1e-8):
+        o = PdhgOptions(tolerance=tol, algorithm=ALGO_HALPERN, check_frequency=64, max_iterations=1_000_000,
+                        device=device)
+        t0 = time.perf_counter()
+        r = PdhgSolver(o).solve(md)
+        dt = time.perf_counter() - t0
+        c = certify(md, r.x, r.y, device)
+        out[f"halpern_{tol:g}"] = {"status": r.status.name, "iterations": r.iterations, "restarts": r.restarts,
+                                   "seconds": dt, "certified_rel_kkt": c.kkt, "certified": bool(c.kkt <= tol * 1.0001),
+                                   "objective": r.objective_value}
+    return out
+
+
+def reference_solvers_section(args, device):
+    """The reference's FP64 CPU solvers (its dual simplex and interior-point
+    method, compiled from its sources into oracle/_ref) on the host cores:
+    the Netlib fixtures and m <= 300 replicas of the plain, precision-ladder
+    and rolling-horizon LPs, each also solved by this library on the GPU
+    (Halpern, 1e-8) to state its error against the FP64 oracle; and one capped
+    attempt at the full-size plain LP.  The reference solvers are single
+    threaded."""
+    import multiprocessing as mp
+
+    import oracle
+    from pramaan_b200 import PdhgOptions, PdhgSolver
+    from pramaan_b200.generators import ill_conditioned_lp, random_sparse_lp, rolling_horizon_lp
+    from pramaan_b200.pdhg import ALGO_HALPERN
+
+    if oracle.ref_cpu() is None:
+        return {"unavailable": "oracle/_ref is not built"}
+    cases = {"cfg0_replica_100x300": random_sparse_lp(100, 300, 4, seed=args.seed),
+             "cfg2_replica_100x250": ill_conditioned_lp(100, 250, 8, seed=args.seed),
+             "cfg3_replica_T24_P5": rolling_horizon_lp(24, 5, seed=args.seed),
+             "cfg3_replica_T48_P5": rolling_horizon_lp(48, 5, seed=args.seed + 1)}
+    mps_dir = REPO / "oracle" / "_ref" / "run" / "tests" / "data"
+    for name in ("afiro", "adlittle"):
+        if (mps_dir / f"{name}.mps").exists():
+            cases[name] = oracle.ref_load_mps(str(mps_dir / f"{name}.mps"))
+    gpu = PdhgSolver(PdhgOptions(tolerance=1e-8, algorithm=ALGO_HALPERN, check_frequency=64,
+                                 max_iterations=1_000_000, device=device))
+    out = {"cores": 1, "host_threads": os.cpu_count(), "tolerance_gpu": 1e-8, "cases": {}}
+    for name, md in cases.items():
+        rec = {"rows": md.numRows(), "cols": md.numVars(), "nnz": int(md.nnz())}
+        best = None
+        for kind in ("dual", "ipm"):
+            t0 = time.perf_counter()
+            try:
+                r = oracle.ref_solve(kind, md, max_iterations=200000, tolerance=1e-9)
+                rec[kind] = {"status": int(r["status"]), "iterations": int(r["iterations"]),
+                             "seconds": time.perf_counter() - t0, "objective": r["objective_value"]}
+                if r["status"] == 0 and best is None:
+                    best = r
+            except Exception as e:   # a reference failure is reported, not raised
+                rec[kind] = {"error": str(e)[:200], "seconds": time.perf_counter() - t0}
+        t0 = time.perf_counter()
+        g = gpu.solve(md)
+        rec["gpu_halpern"] = {"status": g.status.name, "iterations": g.iterations,
+                              "seconds": time.perf_counter() - t0, "objective": g.objective_value}
+        if best is not None:
+            ref_obj = best["objective_value"]
+            rec["oracle_error"] = {
+                "against": "dual simplex" if rec["dual"].get("status") == 0 else "ipm",
+                "objective_rel": abs(g.objective_value - ref_obj) / (1.0 + abs(ref_obj)),
+                "x_inf_rel": float(np.max(np.abs(g.x - best["x"])) / (1.0 + np.max(np.abs(best["x"])))),
+                "note": "x of an LP need not be unique; the objective error is the oracle's measure"}
+        out["cases"][name] = rec
+    # the full-size plain LP under a wall-clock cap, in a child process
+    full = random_sparse_lp(1000, 3000, 4, seed=args.seed)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    proc = ctx.Process(target=_ref_solve_child, args=(full, q))
+    t0 = time.perf_counter()
+    proc.start()
+    proc.join(args.solver_cap_s)
+    if proc.is_alive():
+        proc.terminate()
+        proc.join(10)
+        out["cfg0_full_1000x3000_dual_simplex"] = {"status": "DNF", "cap_s": args.solver_cap_s}
+    else:
+        res = q.get() if not q.empty() else {"status": "no result"}
+        res["seconds"] = time.perf_counter() - t0
+        out["cfg0_full_1000x3000_dual_simplex"] = res
+    return out
+
+
+def _ref_solve_child(md, q):
+    import oracle
+    r = oracle.ref_solve("dual", md, max_iterations=10_000_000, tolerance=1e-9)
+    q.put({"status": int(r["status"]), "iterations": int(r["iterations"]), "objective": r["objective_value"]})
+
+
 def banded_section(args, device):
     """The same iteration on a banded LP of the headline size (2,000,000 x
     5,000,000, 54 columns per row within +-256 of i*n/m): local gathers, so the
@@ -450,11 +592,13 @@ def banded_section(args, device):
             sess.kernel_times(reset=True)
             stream = torch.cuda.ExternalStream(sess.stream(), device=device)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push("timed")
             e0.record(stream)
             for _ in range(args.banded_iters):
                 sess.iterate(1)
             e1.record(stream)
             e1.synchronize()
+            torch.cuda.nvtx.range_pop()
             ms_dual, ms_primal, _ = sess.kernel_times(reset=True)
             b_dual, b_primal = sess.kernel_bytes()
             k = args.banded_iters
@@ -464,6 +608,45 @@ def banded_section(args, device):
                 res[tag] = {"avg_launch_ms": ms / k, "achieved_gbs": gbs, "frac": gbs / hbm}
             out[name] = res
     return out
+
+
+def gnn_section(args, device):
+    """Throughput of the warm-start network on a batch of rolling-horizon LPs
+    with the batched benchmark's shapes (T ~ U{24..336}, P ~ U{5..50}): the
+    forward pass (predict) and one training step (forward + backward + Adam).
+    Dense-layer work per layer and side: 2 * rows * 128 * 64 FLOPs forward,
+    twice that backward (input and weight gradients), and 384 bytes per row
+    forward (a 256-byte BF16 input row read, a 128-byte output row written)."""
+    from pramaan_b200.generators import rolling_horizon_batch
+    from pramaan_b200.gnn import WarmStart, WarmStartNet
+
+    models = rolling_horizon_batch(args.gnn_lps, seed=args.seed)
+    m = sum(md.numRows() for md in models)
+    n = sum(md.numVars() for md in models)
+    rng = np.random.default_rng(args.seed)
+    targets = [WarmStart(rng.uniform(0, 10, md.numVars()), rng.normal(0, 1, md.numRows()), 1.0) for md in models]
+    net = WarmStartNet(device=device, seed=0)
+    t0 = time.perf_counter()
+    g = net.graph(models, targets)
+    t_graph = time.perf_counter() - t0
+    net.predict(g)
+    net.train_step(g, 1e-4)
+    t0 = time.perf_counter()
+    for _ in range(args.gnn_reps):
+        net.predict(g)
+    t_fwd = (time.perf_counter() - t0) / args.gnn_reps
+    t0 = time.perf_counter()
+    for _ in range(args.gnn_reps):
+        net.train_step(g, 1e-4)
+    t_step = (time.perf_counter() - t0) / args.gnn_reps
+    layers = 3
+    fwd_flops = layers * 2 * 128 * 64 * (m + n)
+    return {"workload": f"rolling_horizon_batch {args.gnn_lps} LPs, seed {args.seed}", "rows": m, "cols": n,
+            "nodes": m + n, "nnz": sum(md.nnz() for md in models), "graph_build_s": t_graph,
+            "forward_ms": t_fwd * 1e3, "train_step_ms": t_step * 1e3,
+            "dense_forward_flops": fwd_flops, "dense_train_flops": 3 * fwd_flops,
+            "dense_forward_bytes": layers * 384 * (m + n),
+            "nodes_per_s_forward": (m + n) / t_fwd, "nodes_per_s_train": (m + n) / t_step}
 
 
 def _hints_for(batch, prev):
@@ -501,6 +684,20 @@ def run_gpu_arm(args):
     from pramaan_b200 import PdhgOptions, Session
     from pramaan_b200.generators import model_from_tensors, zipf_lp
 
+    if args.only:
+        sections = {"banded": banded_section, "gnn": gnn_section, "small": small_lp_section,
+                    "stream": learned_stream_section,
+                    "ceiling": lambda a, d: gather_ceiling(a.n, d),
+                    "ladder": ladder_section, "solvers": reference_solvers_section,
+                    "rolling": lambda a, d: rolling_horizon_section(a, d, dist)}
+        out = sections[args.only](args, local)
+        if rank == 0:
+            print(json.dumps({"section": args.only, **out}), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     t = zipf_lp(args.m, args.n, cap=args.cap, seed=args.seed, device=f"cuda:{local}", as_tensors=True)
     model = model_from_tensors(t)
     del t
@@ -522,11 +719,13 @@ def run_gpu_arm(args):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("timed")
         ev0.record(stream)
         for _ in range(args.steps):
             sess.iterate(1)
         ev1.record(stream)
         ev1.synchronize()
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -537,6 +736,12 @@ def run_gpu_arm(args):
         ms = float(tt.item())
     ms_dual, ms_primal, launches = sess.kernel_times(reset=True)
     b_dual, b_primal = sess.kernel_bytes()
+    # The reference checks the FP64 residuals every check_frequency (100)
+    # iterations; the timed steps run none.  Their cost, amortised:
+    t0 = time.perf_counter()
+    for _ in range(5):
+        sess.residuals()
+    check_ms = (time.perf_counter() - t0) / 5 * 1000.0
     sess.close()
     value = world * args.steps / (ms / 1000.0)
 
@@ -553,7 +758,16 @@ def run_gpu_arm(args):
                 "timed_span": "one product: its main kernel and its crossing-row completion kernel"}
     other = [k for k in kinds if k[0] != tag][0]
     roofline["other_kernel"] = {"kernel": other[0], "achieved": other[2] / (other[1] / 1000 / args.steps) / 1e9,
+                                "frac": other[2] / (other[1] / 1000 / args.steps) / 1e9 / hbm,
                                 "avg_launch_ms": other[1] / args.steps}
+    # Second roofline: every non-zero is one random 4-byte gather of x̄ (A x̄)
+    # or y (Aᵀ y, whose hot targets are read from shared memory instead).
+    ceil = gather_ceiling(args.n, local)
+    ceil["per_kernel"] = {}
+    for k_tag, k_ms in (("spmv_dual_fused", ms_dual), ("spmv_primal_fused", ms_primal)):
+        eps = nnz / (k_ms / 1000.0 / args.steps)
+        ceil["per_kernel"][k_tag] = {"entries_per_s": eps, "frac_of_l2_gather_rate": eps / ceil["l2_gathers_per_s"]}
+    roofline["gather_ceiling"] = ceil
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -561,7 +775,11 @@ def run_gpu_arm(args):
             "config": {**workload_config(args, nnz),
                        "gather": gather},
             "gpu_launches": int(launches),
-            "clocks": clk.summary(), "roofline": roofline}
+            "clocks": clk.summary(), "roofline": roofline,
+            "residual_checks": {
+                "note": "the timed steps run no FP64 residual check; the reference checks every 100 iterations",
+                "check_ms": check_ms,
+                "value_with_checks_every_100": world * args.steps / (ms / 1000.0 + args.steps / 100 * check_ms / 1000.0)}}
 
     # ---- end-to-end through the public C ABI with pinned host buffers ----
     if not args.no_e2e:
@@ -585,25 +803,40 @@ def run_gpu_arm(args):
             t0 = time.perf_counter()
             r = solver.solve(pm)
             times.append(time.perf_counter() - t0)
-        e2e_s = max(times) if world == 1 else max(times)
         m, n = model.numRows(), model.numVars()
+        # per call: the LP up (row_ptr, col_idx, values, c, bounds), x, y, the
+        # row activity and the 8 FP64 check scalars of every check down
         h2d = 4 * (m + 1) + 4 * nnz + 8 * nnz + 8 * n + 16 * m + 16 * n
-        d2h = 4 * n + 4 * m + 8 * m + 8 * 8 * (r.checks + 1)
+        d2h = 8 * n + 8 * m + 8 * m + 8 * 8 * (r.checks + 1)
         line["e2e"] = {"value": world * args.e2e_iters / statistics.median(times), "unit": UNIT,
-                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "h2d_bytes_per_step": h2d / args.e2e_iters, "d2h_bytes_per_step": d2h / args.e2e_iters,
+                       "h2d_bytes_per_call": h2d, "d2h_bytes_per_call": d2h,
                        "iterations_per_call": args.e2e_iters, "calls": args.e2e_calls,
-                       "call_s_median": statistics.median(times)}
+                       "call_s_median": statistics.median(times),
+                       "note": "pramaan_pdhg_solve from pinned host buffers, residual checks every 100 "
+                               "iterations; the calls after the warm-up call reuse the library's device-memory "
+                               "cache and its remembered launch shapes (repeated solves of one LP)"}
 
-    if not args.no_banded:
+    # Sections: every rank runs the batched rolling-horizon section (its LPs
+    # shard over the ranks); the single-LP sections are replicas and run on
+    # one GPU only.
+    single = world == 1
+    if single and not args.no_banded:
         line["banded_spmv"] = banded_section(args, local)
-    if not args.no_rolling:
+    if single and not args.no_rolling:
         line["small_lp"] = small_lp_section(args, local)
+    if single and not args.no_ladder:
+        line["ladder_lp"] = ladder_section(args, local)
+    if not args.no_rolling:
         line["rolling_horizon"] = rolling_horizon_section(args, local, dist)
+    if single and not args.no_rolling:
         line["learned_stream"] = learned_stream_section(args, local)
-    if rank == 0 and not args.no_cpu_baseline:
+        line["gnn_throughput"] = gnn_section(args, local)
+    if rank == 0 and single and not args.no_cpu_baseline:
         v, threads, sample = cpu_baseline(model, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": sample}
+                                "sample": sample,
+                                "reference_solvers": reference_solvers_section(args, local)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

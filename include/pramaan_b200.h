@@ -101,12 +101,16 @@ typedef struct pramaan_pdhg_options {
                                  to about 1e-10 are reachable; 0: plain FP32
                                  iterates (resolution about 1e-6)               */
     double reserved_d;
-    int32_t persistent;       /* Halpern mode: 1 runs each check interval as one
-                                 cooperative kernel (grid barriers between the
-                                 products); 0 (default) and -1 launch the two
-                                 products per iteration, captured in a CUDA graph
-                                 with dependent launches (faster on the measured
-                                 operands)                                      */
+    int32_t persistent;       /* Halpern mode, how a check interval runs:
+                                 0 (default): one thread-block cluster per LP
+                                 runs the whole interval in one launch when
+                                 every LP has at most 2^20 non-zeros, else as -1;
+                                 2: the cluster kernel for any size;
+                                 1: one cooperative kernel over the packed
+                                 operand (grid barriers between the products);
+                                 -1: the two tiled products per iteration,
+                                 captured in a CUDA graph with dependent
+                                 launches                                       */
     int32_t gather_cache;     /* 0 (default): the products over a large operand
                                  whose gathers concentrate on few entries (the
                                  transpose of an LP with power-law row lengths)
@@ -416,6 +420,17 @@ PRAMAAN_API int pramaan_session_kernel_bytes(pramaan_pdhg_session* s, double* by
  * per-device cache (at most 32 GB kept per device) so that repeated solves
  * skip cudaMalloc / cudaFree; this returns that memory to the driver. */
 PRAMAAN_API int pramaan_release_cached_memory(int32_t device);
+
+/* Measures the current device's random-gather rate: 4-byte loads of d_x[0, n)
+ * (a device array) at hashed uniform indices, 16 in flight per thread, 8
+ * blocks of 256 threads per SM, nothing else read or written; L1-cached loads
+ * when `cached` is set, else ld.global.cg.  Writes the median over `reps`
+ * timed launches in gathers per second.  The call runs on a stream of its own
+ * and does not wait for other streams: d_x must be ready.  No reference counterpart: it is the
+ * ceiling the benchmark reports the products against, since on a random
+ * sparsity pattern every non-zero costs one such gather. */
+PRAMAAN_API int pramaan_measure_gather_rate(const float* d_x, int32_t n, int32_t cached, int32_t reps,
+                                            double* gathers_per_s);
 
 /* Gather modes (option gather_cache) of the dual product's operand A and the
  * primal product's operand A^T: hot gather slots (entries of x kept in shared

@@ -32,6 +32,8 @@ namespace pb {
 void spmv_noalloc(const int32_t* d_row_ptr, const int32_t* d_col_idx, const float* d_values,
                   int32_t m, int32_t n, int32_t nnz, const float* d_x, float* d_y,
                   cudaStream_t stream);
+// ceiling.cu
+double measure_gather_rate(const float* d_x, int n, bool cached, int reps);
 }  // namespace pb
 
 namespace pb {
@@ -401,6 +403,14 @@ int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual, in
         if (l1_primal) *l1_primal = s->eng->gather_l1_primal();
         if (blocks_dual) *blocks_dual = s->eng->blocks_dual();
         if (blocks_primal) *blocks_primal = s->eng->blocks_primal();
+    });
+}
+
+int pramaan_measure_gather_rate(const float* d_x, int32_t n, int32_t cached, int32_t reps,
+                                double* gathers_per_s) {
+    return guarded([&] {
+        if (!gathers_per_s) throw InvalidArgument("gathers_per_s must not be NULL");
+        *gathers_per_s = measure_gather_rate(d_x, n, cached != 0, reps);
     });
 }
 

@@ -3,9 +3,12 @@
 
 #include "adaptive.cuh"
 #include "adaptive_kernels.cuh"
+#include "cluster_interval.cuh"
 #include "interval.cuh"
 #include "pdhg_engine.cuh"
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -512,6 +515,10 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
 
     preconditioned_steps();          // flat operands: before pack()
     if (opt_.gather_cache >= 0) select_hot_pair(A_, AT_, dev_, st_);
+    // the cluster kernel reads the flat operands (Halpern mode, unless the
+    // graph path or the cooperative kernel is asked for)
+    cluster_ok_ = halpern_ && (opt_.persistent == 0 || opt_.persistent == 2);
+    A_.keep_flat = AT_.keep_flat = cluster_ok_;
     A_.pack(st_);
     AT_.pack(st_);
     // occupancy queries / shared-memory attributes before any graph capture
@@ -551,6 +558,7 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
         }
     }
     apply_steps();
+    if (cluster_ok_) build_cluster_lps();
     PB_CUDA_CHECK(cudaStreamSynchronize(st_));
     // the packed host CSR stays for compaction
     h_rp_ = std::move(rp);
@@ -807,13 +815,101 @@ void AdaptiveBatch::launch_interval(int k) {
     }
 }
 
+// By default (persistent = 0) the cluster kernel takes the intervals once
+// the layout holds few enough LPs for clusters of kClusterAutoMin blocks or
+// more (the tail of a batch, or a single LP) and every LP has at most
+// kClusterAutoMaxNnz non-zeros; persistent = 2 takes it always.  Measured on
+// 128 rolling-horizon LPs: with one block per LP the cluster kernel was 4x
+// slower than the packed tiled products, whose grid spreads every LP over
+// the whole GPU.
+constexpr long long kClusterAutoMaxNnz = 1LL << 20;
+constexpr int kClusterAutoMin = 8;
+
+void AdaptiveBatch::build_cluster_lps() {
+    std::vector<int4> v;
+    long long most = 0;
+    for (const Lp& t : lp_) {
+        if (t.r1 == t.r0 && t.c1 == t.c0) continue;   // not in the current layout
+        v.push_back(make_int4(t.r0, t.r1, t.c0, t.c1));
+        most = std::max(most, t.nnz);
+    }
+    cluster_nlps_ = int(v.size());
+    cluster_auto_ = most <= kClusterAutoMaxNnz;
+    cluster_lps_.alloc(v.size() > 0 ? v.size() : 1);
+    if (!v.empty())
+        PB_CUDA_CHECK(cudaMemcpyAsync(cluster_lps_.get(), v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice, st_));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // v is freed on return
+    // Cluster size: the SMs shared out among the LPs (a power of two, at most
+    // kClusterMax), lowered until the device can hold such a cluster.
+    const int sms = device_sm_count(dev_);
+    int C = 1;
+    while (C * 2 <= kClusterMax && (long long)C * 2 * std::max(cluster_nlps_, 1) <= sms) C *= 2;
+    static std::atomic<int> attr_set[64];
+    const int slot = dev_ >= 0 && dev_ < 64 ? dev_ : 0;
+    if (!attr_set[slot].exchange(1))
+        PB_CUDA_CHECK(cudaFuncSetAttribute(halpern_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    for (; C > 1; C /= 2) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(C));
+        cfg.blockDim = dim3(kClusterThreads);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = unsigned(C);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nc = 0;
+        const cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, halpern_cluster_kernel, &cfg);
+        if (e == cudaSuccess && nc > 0) break;
+        (void)cudaGetLastError();
+    }
+    cluster_size_ = C;
+    cluster_auto_ = cluster_auto_ && C >= kClusterAutoMin;
+}
+
+bool AdaptiveBatch::use_cluster_kernel() const {
+    if (!cluster_ok_ || cluster_nlps_ == 0) return false;
+    return opt_.persistent == 2 || cluster_auto_;
+}
+
+void AdaptiveBatch::launch_cluster(int k) {
+    const int* lpc = K_ == 1 ? nullptr : lp_col_.get();   // one LP: no per-row LP indices
+    const int* lpr = K_ == 1 ? nullptr : lp_row_.get();
+    EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get(), nullptr, lpc,
+                        restart_iter_.get(), iter_base_.get(), 0, nullptr};
+    EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), y_.get(), nullptr, lpr,
+                      restart_iter_.get(), iter_base_.get(), 0, nullptr};
+    const FlatCsr fa{A_.row_ptr.get(), A_.col.get(), A_.val.get()};
+    const FlatCsr fat{AT_.row_ptr.get(), AT_.col.get(), AT_.val.get()};
+    if (n_ > 0 && (!fat.col || !fat.val)) throw std::logic_error("cluster kernel: flat operand missing");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(cluster_nlps_ * cluster_size_));
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.stream = st_;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = unsigned(cluster_size_);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    double *c0 = fpr_c_[0].get(), *c1 = fpr_c_[1].get(), *r0 = fpr_r_[0].get(), *r1 = fpr_r_[1].get();
+    const int4* lps = cluster_lps_.get();
+    const float* yp = y_.get();
+    const float* xb = xbar_.get();
+    PB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, halpern_cluster_kernel, lps, fa, fat, ep, ed, yp, xb, k, c0, c1, r0, r1));
+}
+
 void AdaptiveBatch::iterate(int k, int iter) {
     if (k <= 0) return;
     if (halpern_) {
         set_int_kernel<<<1, 1, 0, st_>>>(iter_base_.get(), iter);
         PB_CUDA_CHECK(cudaGetLastError());
     }
-    if (use_interval_kernel()) {
+    if (use_cluster_kernel()) {
+        launch_cluster(k);
+    } else if (use_interval_kernel()) {
         launch_interval(k);
     } else if (!opt_.use_graph || k > 4096) {
         for (int i = 0; i < k; ++i) iterate_once(i, k);
@@ -1205,8 +1301,15 @@ void AdaptiveBatch::solve_halpern() {
             PB_CUDA_CHECK(cudaMemcpyAsync(restart_iter_.get(), h_restart_iter_, sizeof(int) * K_, cudaMemcpyHostToDevice, st_));
         if (steps_changed) apply_steps();
         long long live = 0;
-        for (const Lp& s : lp_) if (s.active) live += s.nnz;
-        if (live > 0 && 2 * live < (long long)nnz_ && (long long)nnz_ - live >= 65536) compact();
+        int live_lps = 0;
+        for (const Lp& s : lp_) if (s.active) { live += s.nnz; ++live_lps; }
+        // Compact when the LPs still iterating hold less than half of the
+        // operand, or when so few are left that the cluster kernel would take
+        // them alone (clusters of kClusterAutoMin blocks or more).
+        const bool to_cluster = cluster_ok_ && opt_.persistent == 0 && !use_cluster_kernel() && live_lps > 0 &&
+                                live_lps < cluster_nlps_ &&
+                                (long long)live_lps * kClusterAutoMin <= device_sm_count(dev_);
+        if (live > 0 && ((2 * live < (long long)nnz_ && (long long)nnz_ - live >= 65536) || to_cluster)) compact();
     }
     for (Lp& s : lp_)
         if (s.status == PRAMAAN_STATUS_ITERATION_LIMIT) s.iterations = max_it;
@@ -1274,6 +1377,7 @@ void AdaptiveBatch::compact() {
         csr_upload_f64(nA, nm, nn, nnz, rp.data(), ci.data(), val.data(), st_, flag.get());
         csr_transpose(nA, nAT, st_);
         if (opt_.gather_cache >= 0) select_hot_pair(nA, nAT, dev_, st_);
+        nA.keep_flat = nAT.keep_flat = cluster_ok_;
         nA.pack(st_);
         nAT.pack(st_);
         autotune_operand(nA, st_, dev_, status_.get(), opt_.gather_cache);
@@ -1326,6 +1430,7 @@ void AdaptiveBatch::compact() {
     graph_iters_ = 0;
     compacted_ = true;
     ++compactions_;
+    if (cluster_ok_) build_cluster_lps();
 }
 
 void AdaptiveBatch::finish(const pramaan_lp* lps, pramaan_solve_result* results, double solve_ms) {

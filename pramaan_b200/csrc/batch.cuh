@@ -96,6 +96,13 @@ private:
     // Halpern mode on small operands: one cooperative kernel per check interval
     bool use_interval_kernel() const;
     void launch_interval(int k);
+    // Halpern mode, LPs of at most kClusterAutoMaxNnz non-zeros (or on
+    // request): one cluster per LP runs the whole check interval
+    // (cluster_interval.cuh).  build_cluster_lps() lists the LPs of the
+    // current layout and picks the cluster size.
+    bool use_cluster_kernel() const;
+    void build_cluster_lps();
+    void launch_cluster(int k);
     void solve_halpern();
     void materialize_average();
     void push_actions();
@@ -144,6 +151,10 @@ private:
     int* h_restart_iter_ = nullptr;
     DevBuf<double> fpr_c_[2], fpr_r_[2];     // fixed-point residual terms, first / last iteration of an interval
     DevBuf<unsigned> gsync_;                 // grid barrier of the interval kernel {count, generation}
+    bool cluster_ok_ = false;                // flat operands kept, cluster kernel allowed
+    bool cluster_auto_ = false;              // every LP small enough for the automatic choice
+    int cluster_nlps_ = 0, cluster_size_ = 1;
+    DevBuf<int4> cluster_lps_;               // {r0, r1, c0, c1} per LP of the current layout
     DevBuf<double> xw_, yw_;           // warm start (original layout), empty when cold
     DevBuf<double> inv_;
     DevBuf<float> dscale_, pscale_, lp_f_;

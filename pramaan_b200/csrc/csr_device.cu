@@ -3,6 +3,7 @@
 #include "csr_device.cuh"
 #include "epilogues.cuh"
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -413,8 +414,10 @@ void CsrDevice::pack(cudaStream_t st) {
         PB_CUDA_CHECK(cudaStreamSynchronize(st));
     }
     hot_slot.reset();
-    col.reset();
-    val.reset();
+    if (!keep_flat) {
+        col.reset();
+        val.reset();
+    }
     flags.reset();
     meta.reset();
     packed = true;
@@ -604,30 +607,41 @@ void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st) {
 }
 
 // Launch autotuner: picks the resident blocks per SM and the gather mode for
-// one operand by timing the SpMV (store-only epilogue into scratch, so no
-// iterate changes) for every candidate, and records the fastest in the operand.
+// one operand by timing, for every candidate, the product that will run: the
+// caller's fused launch on scratch copies of the vectors it writes, or, when
+// none is given, the store-only product into scratch.  The candidates are
+// timed round-robin, kTuneRepeats times each, and each keeps the median of its
+// repeats, so one noisy burst cannot pick the shape.
 namespace {
 
-// Tuned launch shapes by operand signature, so repeated solves of the same
-// operand (the same LP, or LPs of one generator and size) skip the timing.
+// Tuned launch shapes by operand signature and timed product, so repeated
+// solves of the same operand (the same LP, or LPs of one generator and size)
+// skip the timing.
 struct TuneKey {
-    int dev, rows, cols, nnz, tiles, cross, empty, hot, gather_cache;
+    int dev, rows, cols, nnz, tiles, cross, empty, hot, gather_cache, kind;
     bool operator<(const TuneKey& o) const {
-        return std::tie(dev, rows, cols, nnz, tiles, cross, empty, hot, gather_cache) <
-               std::tie(o.dev, o.rows, o.cols, o.nnz, o.tiles, o.cross, o.empty, o.hot, o.gather_cache);
+        return std::tie(dev, rows, cols, nnz, tiles, cross, empty, hot, gather_cache, kind) <
+               std::tie(o.dev, o.rows, o.cols, o.nnz, o.tiles, o.cross, o.empty, o.hot, o.gather_cache,
+                        o.kind);
     }
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, std::pair<int, int>> g_tuned;   // -> {blocks per SM, gather_l1}
 
+constexpr int kTuneRepeats = 3;         // timed bursts per candidate
+constexpr int kTuneBurst = 5;           // launches per burst
+constexpr float kTuneMargin = 0.98f;    // a later candidate must be 2 % faster
+
 }  // namespace
 
-void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache) {
+void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache,
+                      const TuneLaunch& launch, int kind) {
     using Epi = EpiStore<float, float>;
     using Launch = SpmvLauncher<Epi, float, float, false>;
     A.gather_l1 = (gather_cache > 0 && A.hot == 0) ? 1 : 0;
     if (A.num_tiles < 4 * device_sm_count(dev)) return;   // small operands: default grid
-    const TuneKey key{dev, A.rows, A.cols, A.nnz, A.num_tiles, A.num_cross, A.num_empty, A.hot, gather_cache};
+    if (!launch) kind = 0;
+    const TuneKey key{dev, A.rows, A.cols, A.nnz, A.num_tiles, A.num_cross, A.num_empty, A.hot, gather_cache, kind};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         const auto it = g_tuned.find(key);
@@ -639,39 +653,64 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int g
     }
     const int occ = A.hot > 0 ? Launch::hot_blocks_per_sm(dev) : Launch::blocks_per_sm(dev);
     // L1-cached gathers are a candidate for operands without hot slots; the
-    // L2 mode is timed first and kept unless the other is 2 % faster.
+    // L2 mode comes first and is kept unless the other is 2 % faster.
     const int mode_lo = A.gather_l1;
     const int mode_hi = (gather_cache == 0 && A.hot == 0) ? 1 : A.gather_l1;
-    DevBuf<float> xs(static_cast<size_t>(A.cols > 0 ? A.cols : 1)), ys(static_cast<size_t>(A.rows));
-    PB_CUDA_CHECK(cudaMemsetAsync(xs.get(), 0, xs.bytes(), st));
-    Epi epi{ys.get()};
-    cudaEvent_t e0, e1;
-    PB_CUDA_CHECK(cudaEventCreate(&e0));
-    PB_CUDA_CHECK(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int best_bps = 0, best_mode = mode_lo;
+    DevBuf<float> xs, ys;
+    if (!launch) {
+        xs.alloc(static_cast<size_t>(A.cols > 0 ? A.cols : 1));
+        ys.alloc(static_cast<size_t>(A.rows));
+        PB_CUDA_CHECK(cudaMemsetAsync(xs.get(), 0, xs.bytes(), st));
+    }
+    const Epi epi{ys.get()};
+    auto run = [&](const CsrView& v) {
+        if (launch) launch(v);
+        else Launch::launch(v, xs.get(), epi, status, st, dev);
+    };
+    // Grids above Launch::kTargetBlocks blocks per SM take the dense variants
+    // (operands without hot slots).
+    const int dense = A.hot > 0 ? 0 : Launch::dense_blocks_per_sm(dev);
+    std::vector<std::pair<int, int>> cand;   // {gather mode, blocks per SM}
     for (int mode = mode_lo; mode <= mode_hi; ++mode) {
-        for (int bps = 1; bps <= occ && bps <= 4; ++bps) {
-            A.tuned_blocks_per_sm = bps;
-            A.gather_l1 = mode;
+        for (int bps = 1; bps <= occ && bps <= Launch::kTargetBlocks; ++bps) cand.push_back({mode, bps});
+        for (int bps = Launch::kTargetBlocks + 1; bps <= dense; ++bps) cand.push_back({mode, bps});
+    }
+    std::vector<cudaEvent_t> ev(2 * cand.size() * kTuneRepeats);
+    for (auto& e : ev) PB_CUDA_CHECK(cudaEventCreate(&e));
+    for (const auto& c : cand) {   // warm-up of every shape
+        A.gather_l1 = c.first;
+        A.tuned_blocks_per_sm = c.second;
+        run(A.view(false));
+    }
+    for (int r = 0; r < kTuneRepeats; ++r) {
+        for (size_t k = 0; k < cand.size(); ++k) {
+            A.gather_l1 = cand[k].first;
+            A.tuned_blocks_per_sm = cand[k].second;
             const CsrView v = A.view(false);
-            Launch::launch(v, xs.get(), epi, status, st, dev);   // warm-up
-            PB_CUDA_CHECK(cudaEventRecord(e0, st));
-            for (int r = 0; r < 5; ++r) Launch::launch(v, xs.get(), epi, status, st, dev);
-            PB_CUDA_CHECK(cudaEventRecord(e1, st));
-            PB_CUDA_CHECK(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            PB_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best * 0.98f) { best = ms; best_bps = bps; best_mode = mode; }
+            cudaEvent_t* e = &ev[2 * (k * kTuneRepeats + r)];
+            PB_CUDA_CHECK(cudaEventRecord(e[0], st));
+            for (int b = 0; b < kTuneBurst; ++b) run(v);
+            PB_CUDA_CHECK(cudaEventRecord(e[1], st));
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    float best = 1e30f;
+    int best_bps = 0, best_mode = mode_lo;
+    for (size_t k = 0; k < cand.size(); ++k) {
+        float t[kTuneRepeats];
+        for (int r = 0; r < kTuneRepeats; ++r) {
+            cudaEvent_t* e = &ev[2 * (k * kTuneRepeats + r)];
+            PB_CUDA_CHECK(cudaEventElapsedTime(&t[r], e[0], e[1]));
+        }
+        std::sort(t, t + kTuneRepeats);
+        const float med = t[kTuneRepeats / 2];
+        if (med < best * kTuneMargin) { best = med; best_bps = cand[k].second; best_mode = cand[k].first; }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
     A.tuned_blocks_per_sm = best_bps;
     A.gather_l1 = best_mode;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuned[key] = {best_bps, best_mode};
 }
-
 
 }  // namespace pb

@@ -31,6 +31,7 @@
 #include <atomic>
 #include <stdexcept>
 #include <cstddef>
+#include <functional>
 #include <utility>
 #include <vector>
 
@@ -97,6 +98,8 @@ public:
     int gather_l1 = 0;             // gathers cached in L1 (set by the launch autotuner)
     bool has_lo = false;
     bool packed = false;
+    bool keep_flat = false;        // pack() keeps the flat col / val (FP32) arrays
+                                   // for kernels that read the plain CSR
     DevBuf<int> row_ptr, col, row_map, empty_rows, hot_idx, hot_slot;
     DevBuf<float> val, val_lo;
     DevBuf<uint32_t> flags;
@@ -168,15 +171,20 @@ void select_hot_pair(CsrDevice& A, CsrDevice& AT, int dev, cudaStream_t st);
 // ---------------------------------------------------------------------------
 int device_sm_count(int dev);
 
-// Launch autotuner (results remembered per device and operand signature:
-// shape, crossing and empty rows, hot slots, option): times the store-only
-// product of `A` at 1-4 resident
-// blocks per SM and, for an operand without hot slots, with L2 and with
-// L1-cached gathers, and records the fastest in A.tuned_blocks_per_sm and
-// A.gather_l1 (operands with fewer than 4 tiles per SM keep the default grid
-// and L2 gathers).  gather_cache is the option of that name: -1 keeps L2
-// gathers, 1 takes L1-cached gathers without timing them, 0 times both.
-void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache);
+// Launch autotuner (results remembered per device, operand signature and
+// timed product: shape, crossing and empty rows, hot slots, option, `kind`):
+// times the product of `A` at 1-4 resident blocks per SM and, for an operand
+// without hot slots, with L2 and with L1-cached gathers, and records the
+// fastest median of three bursts in A.tuned_blocks_per_sm and A.gather_l1
+// (operands with fewer than 4 tiles per SM keep the default grid and L2
+// gathers).  `launch`, when given, launches the product that will run (its
+// fused epilogue writing scratch copies of the iterates) for the candidate set
+// in the view; `kind` names it in the remembered results.  Without it the
+// store-only product is timed.  gather_cache is the option of that name: -1
+// keeps L2 gathers, 1 takes L1-cached gathers without timing them, 0 times both.
+using TuneLaunch = std::function<void(const CsrView&)>;
+void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache,
+                      const TuneLaunch& launch = {}, int kind = 0);
 
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp
@@ -243,6 +251,46 @@ struct SpmvLauncher {
     static constexpr int kTargetBlocks =
         int((132 * 1024) / (L::bytes + 1024)) > 0 ? int((132 * 1024) / (L::bytes + 1024)) : 1;
 
+    // Dense variants: the finished rows are staged over the tile's own slots
+    // (no per-warp row buffer), and the carve-out is sized for kDenseBlocks
+    // blocks, so more warps hide the gather and epilogue latencies when the
+    // gathers need less L1 (local operands).  Chosen by a tuned grid of more
+    // than kTargetBlocks blocks per SM.
+    using LD = SpmvSmemLayout<kSpmvWarps, kSpmvStages, kLo, AccT, true>;
+    static constexpr int kDenseBlocks =
+        int((200 * 1024) / (LD::bytes + 1024)) < 6 ? int((200 * 1024) / (LD::bytes + 1024)) : 6;
+    template <bool kRowMap, bool kL1>
+    static constexpr auto dense_kernel() {
+        return &spmv_warp_kernel<Epi, AccT, XT, kLo, kRowMap, kSpmvWarps, kSpmvStages,
+                                 kL1 ? kGatherL1 : kGatherL2, true>;
+    }
+    template <bool kRowMap, bool kL1>
+    static int dense_blocks_per_sm_impl(int dev) {
+        static std::atomic<int> cache[64];
+        if (dev < 0 || dev >= 64) dev = 0;
+        int v = cache[dev].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+        const auto k = dense_kernel<kRowMap, kL1>();
+        PB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LD::bytes)));
+        const long long need = (long long)kDenseBlocks * (LD::bytes + 1024);
+        int pct = int((need * 100 + 228 * 1024 - 1) / (228 * 1024));
+        pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+        PB_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        int nb = 0;
+        PB_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kSpmvWarps * 32, LD::bytes));
+        if (nb < 1) nb = 1;
+        cache[dev].store(nb, std::memory_order_relaxed);
+        return nb;
+    }
+    // Most blocks per SM the dense variants reach (0 when they add none).
+    static int dense_blocks_per_sm(int dev) {
+        dense_blocks_per_sm_impl<true, true>(dev);
+        dense_blocks_per_sm_impl<true, false>(dev);
+        dense_blocks_per_sm_impl<false, true>(dev);
+        const int nb = dense_blocks_per_sm_impl<false, false>(dev);
+        return nb > kTargetBlocks ? nb : 0;
+    }
+
     // kL1: the L1-cached variant (same layout and carve-out as the plain one).
     template <bool kRowMap, bool kL1 = false>
     static int blocks_per_sm_impl(int dev) {
@@ -286,6 +334,7 @@ struct SpmvLauncher {
     // Queries occupancy (and sets the shared-memory attributes) for all
     // variants; call before any stream capture.
     static int blocks_per_sm(int dev) {
+        dense_blocks_per_sm(dev);
         blocks_per_sm_impl<true>(dev);
         blocks_per_sm_impl<true, true>(dev);
         blocks_per_sm_impl<false, true>(dev);
@@ -301,11 +350,17 @@ struct SpmvLauncher {
     // never more than fit, never more blocks than tile groups.
     // For an operand with hot slots the tuned value applies to the FP32 hot
     // kernel (the one the tuner times); the kGatherHotIdx kernels use the default.
+    // True when the launch takes a dense variant.
+    static bool dense_launch(const CsrView& A) { return A.hot == 0 && A.blocks_per_sm > kTargetBlocks; }
     static int grid_for(const CsrView& A, int dev) {
         const bool mapped = A.row_map != nullptr;
         const bool hot = A.hot > 0;
-        const int occ = hot ? (mapped ? hot_blocks_per_sm_impl<true>(dev) : hot_blocks_per_sm_impl<false>(dev))
-                            : (mapped ? blocks_per_sm_impl<true>(dev) : blocks_per_sm_impl<false>(dev));
+        int occ;
+        if (hot) occ = mapped ? hot_blocks_per_sm_impl<true>(dev) : hot_blocks_per_sm_impl<false>(dev);
+        else if (dense_launch(A))
+            occ = mapped ? (A.gather_l1 ? dense_blocks_per_sm_impl<true, true>(dev) : dense_blocks_per_sm_impl<true, false>(dev))
+                         : (A.gather_l1 ? dense_blocks_per_sm_impl<false, true>(dev) : dense_blocks_per_sm_impl<false, false>(dev));
+        else occ = mapped ? blocks_per_sm_impl<true>(dev) : blocks_per_sm_impl<false>(dev);
         int bps;
         if (hot) bps = (kHotMode == kGatherHot && A.blocks_per_sm > 0) ? A.blocks_per_sm : kHotTargetBlocks;
         else bps = A.blocks_per_sm > 0 ? A.blocks_per_sm : kTargetBlocks;
@@ -327,6 +382,15 @@ struct SpmvLauncher {
                     launch_dependent(hot_kernel<true>(), grid, kHotWarps * 32, kHotSmem, st, A, x, epi, dev_status);
                 else
                     launch_dependent(hot_kernel<false>(), grid, kHotWarps * 32, kHotSmem, st, A, x, epi, dev_status);
+            } else if (dense_launch(A)) {
+                const size_t sm = LD::bytes;
+                if (mapped) {
+                    if (A.gather_l1) launch_dependent(dense_kernel<true, true>(), grid, kSpmvWarps * 32, sm, st, A, x, epi, dev_status);
+                    else launch_dependent(dense_kernel<true, false>(), grid, kSpmvWarps * 32, sm, st, A, x, epi, dev_status);
+                } else {
+                    if (A.gather_l1) launch_dependent(dense_kernel<false, true>(), grid, kSpmvWarps * 32, sm, st, A, x, epi, dev_status);
+                    else launch_dependent(dense_kernel<false, false>(), grid, kSpmvWarps * 32, sm, st, A, x, epi, dev_status);
+                }
             } else if (A.gather_l1) {
                 if (mapped)
                     launch_dependent(l1_kernel<true>(), grid, kSpmvWarps * 32, L::bytes, st, A, x, epi, dev_status);

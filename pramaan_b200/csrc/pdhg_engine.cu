@@ -125,7 +125,7 @@ void validate_options(const pramaan_pdhg_options& opt) {
         throw InvalidArgument("pdhg options: the adaptive and Halpern algorithms terminate on the relative KKT "
                               "error (PRAMAAN_TERM_RELATIVE_KKT)");
     if (opt.refine != 0 && opt.refine != 1) throw InvalidArgument("pdhg options: refine must be 0 or 1");
-    if (opt.persistent < -1 || opt.persistent > 1) throw InvalidArgument("pdhg options: persistent must be -1, 0 or 1");
+    if (opt.persistent < -1 || opt.persistent > 2) throw InvalidArgument("pdhg options: persistent must be -1, 0, 1 or 2");
     if (opt.gather_cache < -1 || opt.gather_cache > 1) throw InvalidArgument("pdhg options: gather_cache must be -1, 0 or 1");
     if (opt.algorithm == PRAMAAN_ALGO_HALPERN && opt.refine != 1)
         throw InvalidArgument("pdhg options: the Halpern algorithm runs on FP64 master iterates (refine = 1)");
@@ -211,10 +211,30 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     SpmvLauncher<EpiStore<double, double>, double, float, true>::blocks_per_sm(dev_);
     SpmvLauncher<EpiStore<double, double>, double, float, false>::blocks_per_sm(dev_);
     SpmvLauncher<EpiStore<float, float>, float, float, false>::blocks_per_sm(dev_);
-    // The FP32 product kernels share one shared-memory layout, so the grid the
-    // tuner picks for the store-only kernel carries over to the PDHG epilogues.
-    autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache);
-    autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache);
+    if (!adaptive_) {
+        // The tuner times the fused products of the reference iteration
+        // themselves, writing scratch copies of y, x and x̄.
+        DevBuf<float> ys(size_t(m_ > 0 ? m_ : 1)), xs(size_t(n_ > 0 ? n_ : 1)), xbs(size_t(n_ > 0 ? n_ : 1));
+        if (m_ > 0) PB_CUDA_CHECK(cudaMemcpyAsync(ys.get(), y_.get(), size_t(m_) * 4, cudaMemcpyDeviceToDevice, st_));
+        if (n_ > 0) {
+            PB_CUDA_CHECK(cudaMemcpyAsync(xs.get(), x_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
+            PB_CUDA_CHECK(cudaMemcpyAsync(xbs.get(), xbar_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
+        }
+        const EpiDualRef de{sigma_.get(), lr_.get(), ur_.get(), ys.get()};
+        const EpiPrimalRef pe{tau_.get(), c_.get(), lx_.get(), ux_.get(), xs.get(), xbs.get()};
+        autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
+            SpmvLauncher<EpiDualRef, float, float, false>::launch(v, xbar_.get(), de, status_.get(), st_, dev_);
+        }, /*kind=*/1);
+        autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
+            SpmvLauncher<EpiPrimalRef, float, float, false>::launch(v, y_.get(), pe, status_.get(), st_, dev_);
+        }, /*kind=*/2);
+        PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // scratch copies are freed on return
+    } else {
+        // The FP32 product kernels share one shared-memory layout, so the grid the
+        // tuner picks for the store-only kernel carries over to the adaptive epilogues.
+        autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache);
+        autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache);
+    }
     if (adaptive_) {
         SpmvLauncher<EpiDualAdapt, float, float, false>::blocks_per_sm(dev_);
         SpmvLauncher<EpiPrimalAdapt, float, float, false>::blocks_per_sm(dev_);

@@ -220,12 +220,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // kG: gather mode (spmv_gather).  With kGatherHot the block's copy of the
 // hot targets sits after the rings (shared-memory offset L::bytes, A.hot
 // values of XT).
+// kStageAlias: stage the finished rows over the tile's column / value slots
+// in any gather mode (the hot-slot mode always does), so a warp needs only its
+// ring and more warps fit on an SM.
 template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kG = kGatherL2,
-          class Ready>
+          bool kStageAlias = false, class Ready>
 __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restrict__ x, const Epi& epi,
                                            int* __restrict__ dev_status, unsigned char* smem, uint32_t& used,
                                            bool init_bars, Ready&& ready) {
-    constexpr bool kAlias = kG == kGatherHot;
+    constexpr bool kAlias = kG == kGatherHot || kStageAlias;
     using L = SpmvSmemLayout<WARPS, STAGES, kLo, AccT, kAlias>;
     constexpr int IPT = kSpmvIpt;
     constexpr int TW = L::TW;
@@ -457,14 +460,15 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
     return !failed;
 }
 
-template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kG = kGatherL2>
+template <class Epi, typename AccT, typename XT, bool kLo, bool kRowMap, int WARPS, int STAGES, int kG = kGatherL2,
+          bool kStageAlias = false>
 __global__ void __launch_bounds__(WARPS * 32, (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS > 0
                                                   ? (sizeof(AccT) == 4 ? 5 : 4) * 4 / WARPS : 1)
     spmv_warp_kernel(const CsrView A, const XT* __restrict__ x, const Epi epi,
                      int* __restrict__ dev_status) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t used = 0;
-    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES, kG>(A, x, epi, dev_status, smem, used, true, [] {
+    spmv_tiles<Epi, AccT, XT, kLo, kRowMap, WARPS, STAGES, kG, kStageAlias>(A, x, epi, dev_status, smem, used, true, [] {
         grid_dep_launch();
         grid_dep_wait();
         return true;

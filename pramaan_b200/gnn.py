@@ -203,17 +203,47 @@ class WarmSolveInfo:
     certify_s: float
     solve_s: float
     fallback_s: float
+    probe_iterations: int = 0   # iterations spent on the probes, all candidates counted
 
 
-def select_starts(models: list[ModelIR], candidates: dict[str, list], device: int = 0):
+def probe_candidates(models: list[ModelIR], sets: list[list], options: PdhgOptions, iterations: int):
+    """Runs `iterations` PDHG iterations from every candidate start of every LP
+    (one batch of all of them) and returns the points reached, per candidate
+    set, with None kept for candidates that do not exist."""
+    o = dataclasses.replace(options, tolerance=0.0, max_iterations=iterations,
+                            check_frequency=min(options.check_frequency, iterations))
+    flat, where = [], []
+    for p, st in enumerate(sets):
+        for i, w in enumerate(st):
+            if w is not None or p == len(sets) - 1:   # the last set (cold) is always probed
+                flat.append(i)
+                where.append((p, i, w))
+    res = solve_batch([models[i] for i in flat], o, warm=[w for _, _, w in where])
+    out = [[None] * len(models) for _ in sets]
+    for (p, i, _), r in zip(where, res):
+        out[p][i] = WarmStart(r.x, r.y, 0.0)
+    return out, len(flat) * iterations
+
+
+def select_starts(models: list[ModelIR], candidates: dict[str, list], device: int = 0,
+                  probe_iterations: int = 0, options: PdhgOptions | None = None):
     """The certificate decides: for every LP, the candidate start with the
     smallest FP64 relative KKT error (max of primal, dual and gap) among
     ``candidates`` (name -> one point or None per LP), with the cold start
-    always among them.  Returns (starts, names, kkt)."""
+    always among them.  With ``probe_iterations`` > 0 every candidate is first
+    advanced that many PDHG iterations (``options``) and judged, and returned,
+    at the point it reached: a start whose error is small but whose
+    neighbourhood converges slowly loses to one that moves faster.  Returns
+    (starts, names, kkt, probe iterations spent)."""
     from .certificate import certify_batch
 
     names = list(candidates) + ["cold"]
     sets = [candidates[nm] for nm in candidates] + [[None] * len(models)]
+    spent = 0
+    if probe_iterations > 0:
+        if options is None:
+            raise ValueError("select_starts: probing needs the solver options")
+        sets, spent = probe_candidates(models, sets, options, probe_iterations)
     certs = certify_batch(models, sets, device)
     starts, chosen, kkt = [], [], []
     for i in range(len(models)):
@@ -224,20 +254,24 @@ def select_starts(models: list[ModelIR], candidates: dict[str, list], device: in
         starts.append(sets[best][i])
         chosen.append(names[best])
         kkt.append(certs[best][i].kkt)
-    return starts, chosen, kkt
+    return starts, chosen, kkt, spent
 
 
 def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOptions,
                      fallback_iterations: int | None = None,
                      hints: list[WarmStart | None] | None = None,
-                     use_predicted_weight: bool = False) -> tuple[list[SolveResult], WarmSolveInfo]:
+                     use_predicted_weight: bool = False,
+                     probe_iterations: int = 0) -> tuple[list[SolveResult], WarmSolveInfo]:
     """Learned warm start, certified, with the cold start as fallback.
 
     1. The network predicts (x, y, omega) for every LP (refining ``hints``
        when given, see ``GnnGraph``).
     2. The certificate decides the start of each LP: the network's point, the
        hint or the cold start, whichever has the smallest FP64 relative KKT
-       error (``select_starts``).
+       error (``select_starts``), judged after ``probe_iterations`` PDHG
+       iterations from each when that is > 0 (the solve then continues from
+       the chosen probe's point; every probe's iterations are counted in
+       ``WarmSolveInfo.probe_iterations``).
     3. The batch is solved from those starts (with the predicted primal
        weight when ``use_predicted_weight``, else the solver's default).
     4. Every LP whose solve is not optimal (it hit ``options.max_iterations``)
@@ -252,7 +286,7 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
     cands = {"network": pred}
     if hints is not None:
         cands["hint"] = list(hints)
-    starts, chosen, kkt = select_starts(models, cands, net.device)
+    starts, chosen, kkt, spent = select_starts(models, cands, net.device, probe_iterations, options)
     warm = []
     for st, nm, p in zip(starts, chosen, pred):
         if st is None:
@@ -274,4 +308,4 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
             if r.status == SolveStatus.kOptimal or res[i].status != SolveStatus.kOptimal:
                 res[i] = r
     t4 = time.perf_counter()
-    return res, WarmSolveInfo(warm_its, chosen, kkt, len(bad), t1 - t0, t2 - t1, t3 - t2, t4 - t3)
+    return res, WarmSolveInfo(warm_its, chosen, kkt, len(bad), t1 - t0, t2 - t1, t3 - t2, t4 - t3, spent)

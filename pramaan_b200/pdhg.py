@@ -128,8 +128,10 @@ class PdhgOptions:
     use_graph: bool = True
     profile_kernels: bool = False
     refine: bool = True         # adaptive mode: FP64 master iterates + FP32 corrections
-    persistent: int = 0         # Halpern mode: 1 one cooperative kernel per check interval,
-                                # 0 / -1 two dependent launches per iteration in a CUDA graph
+    persistent: int = 0         # Halpern mode: 0 one cluster per LP runs each check interval when every LP
+                                # has <= 2^20 non-zeros (else -1), 2 the cluster kernel always,
+                                # 1 one cooperative kernel per interval, -1 two dependent launches
+                                # per iteration in a CUDA graph
     gather_cache: int = 0       # 0: hot gather targets of large skewed operands in shared memory and
                                 # L1-cached gathers where the autotuner finds them faster;
                                 # 1: L1-cached gathers on every operand without hot slots; -1: plain

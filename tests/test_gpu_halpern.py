@@ -108,3 +108,60 @@ def test_interval_kernel_matches_the_per_kernel_path_bit_for_bit():
     single_g = PdhgSolver(PdhgOptions(tolerance=1e-7, max_iterations=200000, check_frequency=37,
                                       algorithm=ALGO_HALPERN, persistent=-1)).solve(models[5])
     assert single.iterations == single_g.iterations and np.array_equal(single.x, single_g.x)
+
+
+def _with_empty_row():
+    from pramaan_b200.pdhg import ModelIR
+    return ModelIR([1.0, 2.0, 1.0], [0, 2, 2, 4], [0, 1, 1, 2], [1.0, 1.0, 1.0, -1.0],
+                   [1.0, -1e30, -2.0], [4.0, 5.0, 2.0], [0.0, 0.0, 0.0], [3.0, 3.0, 3.0], 0, 0.0)
+
+
+def test_cluster_kernel_follows_the_tiled_path():
+    """One thread-block cluster per LP running whole check intervals
+    (persistent = 2) against the tiled products in a CUDA graph
+    (persistent = -1).  Both apply the same per-element updates; the cluster
+    kernel sums each row in CSR order, which the tiled kernel also does for a
+    row inside one tile, so over one check interval (no restart yet) the
+    iterates agree to FP32 rounding, and complete solves reach the same
+    certified answers."""
+    models = rolling_horizon_batch(5, seed=6, T_range=(24, 60), P_range=(5, 10)) + [
+        random_sparse_lp(300, 900, 4, seed=2), _with_empty_row()]
+    short = dict(tolerance=0.0, max_iterations=64, check_frequency=64, algorithm=ALGO_HALPERN)
+    a = solve_batch(models, PdhgOptions(persistent=2, **short))
+    b = solve_batch(models, PdhgOptions(persistent=-1, **short))
+    for ra, rb in zip(a, b):
+        assert ra.iterations == rb.iterations == 64
+        assert np.allclose(ra.x, rb.x, rtol=1e-4, atol=1e-4 * (1 + np.abs(rb.x).max()))
+        assert np.allclose(ra.y, rb.y, rtol=1e-4, atol=1e-4 * (1 + np.abs(rb.y).max()))
+    full = dict(tolerance=1e-7, max_iterations=200000, check_frequency=64, algorithm=ALGO_HALPERN)
+    a = solve_batch(models, PdhgOptions(persistent=2, **full))
+    b = solve_batch(models, PdhgOptions(persistent=-1, **full))
+    for md, ra, rb in zip(models, a, b):
+        assert ra.status == rb.status == SolveStatus.kOptimal
+        k = oracle.rel_kkt(md, ra.x, ra.y)
+        assert max(k["primal"], k["dual"], k["gap"]) <= 1e-7 * 1.0001
+        assert ra.objective_value == pytest.approx(rb.objective_value, rel=1e-5, abs=1e-5)
+        assert ra.iterations <= 2 * rb.iterations + 256 and rb.iterations <= 2 * ra.iterations + 256
+    again = solve_batch(models, PdhgOptions(persistent=2, **full))
+    for ra, rc in zip(a, again):   # deterministic run to run
+        assert ra.iterations == rc.iterations and np.array_equal(ra.x, rc.x) and np.array_equal(ra.y, rc.y)
+
+
+def test_cluster_kernel_single_lp_and_one_lp_left():
+    """A single LP (a batch of one gets the largest cluster) and a batch whose
+    compaction leaves one slow LP alone: answers certified and equal to the
+    tiled path's within the tolerance's reach."""
+    md = random_sparse_lp(1000, 3000, 4, seed=0)
+    full = dict(tolerance=1e-8, max_iterations=400000, check_frequency=64, algorithm=ALGO_HALPERN)
+    r = PdhgSolver(PdhgOptions(persistent=2, **full)).solve(md)
+    g = PdhgSolver(PdhgOptions(persistent=-1, **full)).solve(md)
+    assert r.status == g.status == SolveStatus.kOptimal
+    k = oracle.rel_kkt(md, r.x, r.y)
+    assert max(k["primal"], k["dual"], k["gap"]) <= 1e-8 * 1.0001
+    assert r.objective_value == pytest.approx(g.objective_value, rel=1e-7, abs=1e-7)
+    models = [rolling_horizon_lp(24, 5, seed=s) for s in range(6)] + [rolling_horizon_lp(96, 20, seed=7)]
+    res = solve_batch(models, PdhgOptions(persistent=2, **dict(full, tolerance=1e-6)))
+    for m_, rr in zip(models, res):
+        assert rr.status == SolveStatus.kOptimal
+        kk = oracle.rel_kkt(m_, rr.x, rr.y)
+        assert max(kk["primal"], kk["dual"], kk["gap"]) <= 1e-6 * 1.0001
