@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="reference arm: skip timing the reference's own GPU solver")
     p.add_argument("--rh-count", type=int, default=512,
                    help="LPs of the batched rolling-horizon section (the published batch: 512)")
     p.add_argument("--ladder-m", type=int, default=200_000, help="rows of the precision-ladder LP")
@@ -77,6 +79,9 @@ def parse():
     p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
     p.add_argument("--no-banded", action="store_true", help="skip the banded-LP bandwidth section")
     p.add_argument("--banded-iters", type=int, default=50)
+    p.add_argument("--launch-blocks", type=int, default=0,
+                   help="fixed blocks per SM of the products (0: autotuned); with --gather-cache 1 or -1 "
+                        "the launch shape is fixed, for profiles")
     p.add_argument("--only", default=None, choices=["banded", "gnn", "small", "rolling", "stream", "ceiling", "ladder", "solvers"],
                    help="run one section alone on the given sizes and print its JSON (profiling runs)")
     p.add_argument("--gnn-lps", type=int, default=64, help="rolling-horizon LPs of the network throughput section")
@@ -282,7 +287,42 @@ def run_reference_arm(args):
                              "sample": f"{args.steps} full iterations (the reference has no CPU PDHG; "
                                        "its algorithm restated in C, OpenMP over rows/columns)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if torch.cuda.is_available() and not args.no_reference_gpu:
+        torch.cuda.empty_cache()
+        line["reference_gpu"] = reference_gpu_section(args, model)
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_section(args, model):
+    """The reference's own GPU PDHG (src/gpu/pdhg_solver.cu, compiled for
+    sm_100a into oracle/_ref), reported beside this library: iterations/s on
+    the same 2 M x 5 M LP (difference of a 300- and a 100-iteration solve,
+    each with its FP64 host check every 100 iterations, so setup cancels and
+    the checks are counted as the reference runs them) and time to its 1e-4
+    criterion on the 1000 x 3000 plain LP."""
+    import oracle
+    from pramaan_b200.generators import random_sparse_lp
+
+    if oracle.ref_gpu() is None:
+        return {"unavailable": "oracle/_ref/libref_gpu.so is not built"}
+    out = {"source": "src/gpu/pdhg_solver.cu (PdhgSolver::solve), nvcc -gencode arch=compute_100a,code=sm_100a"}
+    with ClockSampler(0) as clk:
+        times = {}
+        for iters in (100, 300):
+            t0 = time.perf_counter()
+            r = oracle.ref_solve("pdhg", model, max_iterations=iters, tolerance=0.0, check_frequency=100)
+            times[iters] = time.perf_counter() - t0
+        small = random_sparse_lp(1000, 3000, 4, seed=args.seed)
+        oracle.ref_solve("pdhg", small, max_iterations=200, tolerance=1e-4, check_frequency=100)
+        t0 = time.perf_counter()
+        rs = oracle.ref_solve("pdhg", small, max_iterations=100000, tolerance=1e-4, check_frequency=100)
+        t_small = time.perf_counter() - t0
+    out[WORKLOAD] = {"iterations_per_s": 200.0 / (times[300] - times[100]), "solve_100_s": times[100],
+                     "solve_300_s": times[300], "status_300": int(r["status"])}
+    out["random_sparse_lp_1000x3000_to_1e-4"] = {"seconds": t_small, "iterations": int(rs["iterations"]),
+                                                 "status": int(rs["status"]), "objective": rs["objective_value"]}
+    out["clocks"] = clk.summary()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -583,9 +623,10 @@ def banded_section(args, device):
     hbm, kind = measured_peaks()
     out = {"workload": f"banded_lp {args.m} x {args.n}, 54 per row, band 256, seed {args.seed}",
            "nnz": int(model.nnz()), "peak_gbs": hbm, "peak_kind": kind, "iterations": args.banded_iters}
-    for name, cache in (("auto", 0), ("l2_gathers", -1)):
+    modes = (("auto", args.gather_cache), ("l2_gathers", -1)) if args.gather_cache != -1 else (("l2_gathers", -1),)
+    for name, cache in modes:
         with Session(model, PdhgOptions(device=device, use_graph=False, profile_kernels=True,
-                                        gather_cache=cache)) as sess:
+                                        gather_cache=cache, launch_blocks=args.launch_blocks)) as sess:
             for _ in range(3):
                 sess.iterate(1)
             sess.synchronize()
@@ -704,7 +745,8 @@ def run_gpu_arm(args):
     torch.cuda.empty_cache()
     nnz = model.nnz()
 
-    opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True, gather_cache=args.gather_cache)
+    opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True, gather_cache=args.gather_cache,
+                       launch_blocks=args.launch_blocks)
     sess = Session(model, opts)
     gather = sess.gather_info()
     stream = torch.cuda.ExternalStream(sess.stream(), device=local)

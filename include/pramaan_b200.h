@@ -121,7 +121,14 @@ typedef struct pramaan_pdhg_options {
                                  L1-cached gathers on every operand without hot
                                  entries; -1: plain L2 gathers only.  The
                                  results are identical in every mode            */
-    int32_t reserved[4];
+    int32_t launch_blocks;    /* 0 (default): the launch autotuner picks the
+                                 resident blocks per SM of the products over a
+                                 large operand; > 0: that many (capped by what
+                                 fits), only the gather mode is then timed,
+                                 and not even that when gather_cache is 1 or
+                                 -1: a fixed launch shape, for reproducible
+                                 profiles                                       */
+    int32_t reserved[3];
 } pramaan_pdhg_options;
 
 /* Result, mirroring pramaan::SolveResult (include/pramaan/simplex.hpp:40-76).

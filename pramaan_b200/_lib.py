@@ -36,7 +36,7 @@ class COptions(C.Structure):
         ("tolerance", f64), ("max_iterations", i32), ("check_frequency", i32),
         ("algorithm", i32), ("termination", i32), ("device", i32), ("use_graph", i32),
         ("profile_kernels", i32), ("refine", i32), ("reserved_d", f64),
-        ("persistent", i32), ("gather_cache", i32), ("reserved", i32 * 4),
+        ("persistent", i32), ("gather_cache", i32), ("launch_blocks", i32), ("reserved", i32 * 3),
     ]
 
 

@@ -531,8 +531,8 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     warm_launcher<EpiStore<double, double>, double, double>(dev_);
     warm_launcher<EpiRowViolOut, double, double>(dev_);
     warm_launcher<EpiColResidOut, double, double>(dev_);
-    autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache);
-    autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache);
+    autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
+    autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
     estimate_step_sizes();
 
     // initial primal weight per LP: ||C c|| / ||R b|| on the scaled LP
@@ -816,14 +816,17 @@ void AdaptiveBatch::launch_interval(int k) {
 }
 
 // By default (persistent = 0) the cluster kernel takes the intervals once
-// the layout holds few enough LPs for clusters of kClusterAutoMin blocks or
-// more (the tail of a batch, or a single LP) and every LP has at most
+// the layout holds few enough LPs for clusters of kClusterAutoMin blocks (the
+// tail of a batch, or a single LP) and every LP has at most
 // kClusterAutoMaxNnz non-zeros; persistent = 2 takes it always.  Measured on
-// 128 rolling-horizon LPs: with one block per LP the cluster kernel was 4x
-// slower than the packed tiled products, whose grid spreads every LP over
-// the whole GPU.
+// the rolling-horizon batch (128 LPs, T ~ U{24..336}, P ~ U{5..50}): its
+// slowest LP alone (66,704 non-zeros, 300 k iterations) at 16.9 us per
+// iteration against 19.5 on the tiled path, its 2 and 5 slowest LPs at 17.9 /
+// 20.5 against 22.2 / 24.9 us; with one block per LP (the whole batch) the
+// cluster kernel was 4x slower than the packed tiled products, whose grid
+// spreads every LP over the whole GPU.
 constexpr long long kClusterAutoMaxNnz = 1LL << 20;
-constexpr int kClusterAutoMin = 8;
+constexpr int kClusterAutoMin = 16;
 
 void AdaptiveBatch::build_cluster_lps() {
     std::vector<int4> v;
@@ -1380,8 +1383,8 @@ void AdaptiveBatch::compact() {
         nA.keep_flat = nAT.keep_flat = cluster_ok_;
         nA.pack(st_);
         nAT.pack(st_);
-        autotune_operand(nA, st_, dev_, status_.get(), opt_.gather_cache);
-        autotune_operand(nAT, st_, dev_, status_.get(), opt_.gather_cache);
+        autotune_operand(nA, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
+        autotune_operand(nAT, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
     }
 
     // 4. the first compaction keeps the original layout for the final evaluation

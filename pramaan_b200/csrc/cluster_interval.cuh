@@ -15,7 +15,8 @@
 //
 // The products read the flat FP32 CSR of A and of A^T (the operand the tile
 // records were packed from): one thread per row (kRowsPerPass rows of a thread
-// advanced together), entries in CSR order, one FMA each, so a row's sum has the order the tiled kernel uses for a row inside
+// advanced together, kEntryChunk entries at a time), entries in CSR order, one
+// FMA each, so a row's sum has the order the tiled kernel uses for a row inside
 // one tile.  The vector updates are the same epilogue objects as the tiled
 // path (same arithmetic per element).  The gathers of y and x̄, written by the
 // other blocks of the cluster, are ld.global.cg loads after the cluster
@@ -58,15 +59,21 @@ __device__ __forceinline__ void cluster_barrier() {
 }
 
 // Rows r_u = r0 + u * step (u < kRowsPerPass, those below r_end) of a flat
-// CSR times x, into acc[u]: each row's entries in order, one FMA each, the
-// rows' loads interleaved so that their latencies overlap.  x is read past
-// L1 (other SMs of the cluster wrote it); the operand is read-only for the
-// kernel and may stay in L1.
-constexpr int kRowsPerPass = 4;
+// CSR times x, into acc[u]: each row's entries in CSR order, one FMA each.
+// The entries are loaded kEntryChunk at a time for every row of the pass
+// before any of them is summed, so one chunk costs one round trip of
+// dependent loads (column index, then x) whatever the row lengths, and long
+// rows (a capacity row touches every product of its period) take
+// ceil(length / kEntryChunk) round trips instead of one per entry.  x is
+// read past L1 (other SMs of the cluster wrote it); the operand is read-only
+// for the kernel.
+constexpr int kRowsPerPass = 2;
+constexpr int kEntryChunk = 8;
 
 __device__ __forceinline__ void flat_rows_dot(const FlatCsr& A, const float* __restrict__ x, int r0, int step,
                                               int r_end, float (&acc)[kRowsPerPass]) {
     int e[kRowsPerPass], e1[kRowsPerPass];
+    bool more = false;
 #pragma unroll
     for (int u = 0; u < kRowsPerPass; ++u) {
         const int r = r0 + u * step;
@@ -74,25 +81,32 @@ __device__ __forceinline__ void flat_rows_dot(const FlatCsr& A, const float* __r
         e[u] = ok ? __ldg(A.row_ptr + r) : 0;
         e1[u] = ok ? __ldg(A.row_ptr + r + 1) : 0;
         acc[u] = 0.0f;
+        more = more || e[u] < e1[u];
     }
-    bool more = true;
     while (more) {
-        more = false;
-        float v[kRowsPerPass], xv[kRowsPerPass];
+        float v[kRowsPerPass][kEntryChunk], xv[kRowsPerPass][kEntryChunk];
+        int c[kRowsPerPass][kEntryChunk];
 #pragma unroll
-        for (int u = 0; u < kRowsPerPass; ++u) {
-            const bool ok = e[u] < e1[u];
-            const int c = ok ? __ldg(A.col + e[u]) : 0;
-            v[u] = ok ? __ldg(A.val + e[u]) : 0.0f;
-            xv[u] = ok ? __ldcg(x + c) : 0.0f;
-        }
+        for (int u = 0; u < kRowsPerPass; ++u)
 #pragma unroll
-        for (int u = 0; u < kRowsPerPass; ++u) {
-            if (e[u] < e1[u]) {
-                acc[u] = fmaf(v[u], xv[u], acc[u]);
-                ++e[u];
-                more = more || e[u] < e1[u];
+            for (int k = 0; k < kEntryChunk; ++k) {
+                const bool ok = e[u] + k < e1[u];
+                c[u][k] = ok ? __ldg(A.col + e[u] + k) : 0;
+                v[u][k] = ok ? __ldg(A.val + e[u] + k) : 0.0f;
             }
+#pragma unroll
+        for (int u = 0; u < kRowsPerPass; ++u)
+#pragma unroll
+            for (int k = 0; k < kEntryChunk; ++k)
+                xv[u][k] = e[u] + k < e1[u] ? __ldcg(x + c[u][k]) : 0.0f;
+        more = false;
+#pragma unroll
+        for (int u = 0; u < kRowsPerPass; ++u) {
+#pragma unroll
+            for (int k = 0; k < kEntryChunk; ++k)
+                if (e[u] + k < e1[u]) acc[u] = fmaf(v[u][k], xv[u][k], acc[u]);
+            e[u] += kEntryChunk;
+            more = more || e[u] < e1[u];
         }
     }
 }

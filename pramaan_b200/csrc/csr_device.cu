@@ -635,13 +635,14 @@ constexpr float kTuneMargin = 0.98f;    // a later candidate must be 2 % faster
 }  // namespace
 
 void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache,
-                      const TuneLaunch& launch, int kind) {
+                      const TuneLaunch& launch, int kind, int launch_blocks) {
     using Epi = EpiStore<float, float>;
     using Launch = SpmvLauncher<Epi, float, float, false>;
     A.gather_l1 = (gather_cache > 0 && A.hot == 0) ? 1 : 0;
     if (A.num_tiles < 4 * device_sm_count(dev)) return;   // small operands: default grid
     if (!launch) kind = 0;
-    const TuneKey key{dev, A.rows, A.cols, A.nnz, A.num_tiles, A.num_cross, A.num_empty, A.hot, gather_cache, kind};
+    const TuneKey key{dev, A.rows, A.cols, A.nnz, A.num_tiles, A.num_cross, A.num_empty, A.hot, gather_cache,
+                      kind * 64 + (launch_blocks > 0 ? launch_blocks : 0)};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         const auto it = g_tuned.find(key);
@@ -672,8 +673,20 @@ void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int g
     const int dense = A.hot > 0 ? 0 : Launch::dense_blocks_per_sm(dev);
     std::vector<std::pair<int, int>> cand;   // {gather mode, blocks per SM}
     for (int mode = mode_lo; mode <= mode_hi; ++mode) {
+        if (launch_blocks > 0) {   // a fixed shape: the largest grid up to the request that fits
+            const int top = std::max(std::min(occ, Launch::kTargetBlocks), dense);
+            cand.push_back({mode, std::min(launch_blocks, top)});
+            continue;
+        }
         for (int bps = 1; bps <= occ && bps <= Launch::kTargetBlocks; ++bps) cand.push_back({mode, bps});
         for (int bps = Launch::kTargetBlocks + 1; bps <= dense; ++bps) cand.push_back({mode, bps});
+    }
+    if (cand.size() == 1) {   // nothing to time
+        A.gather_l1 = cand[0].first;
+        A.tuned_blocks_per_sm = cand[0].second;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[key] = {cand[0].second, cand[0].first};
+        return;
     }
     std::vector<cudaEvent_t> ev(2 * cand.size() * kTuneRepeats);
     for (auto& e : ev) PB_CUDA_CHECK(cudaEventCreate(&e));

@@ -183,8 +183,10 @@ int device_sm_count(int dev);
 // store-only product is timed.  gather_cache is the option of that name: -1
 // keeps L2 gathers, 1 takes L1-cached gathers without timing them, 0 times both.
 using TuneLaunch = std::function<void(const CsrView&)>;
+// launch_blocks > 0 fixes the blocks per SM (capped by what fits): only the
+// gather modes are timed, and nothing when there is one candidate.
 void autotune_operand(CsrDevice& A, cudaStream_t st, int dev, int* status, int gather_cache,
-                      const TuneLaunch& launch = {}, int kind = 0);
+                      const TuneLaunch& launch = {}, int kind = 0, int launch_blocks = 0);
 
 constexpr int kSpmvWarps = 4;     // warps per block (each with its own ring)
 constexpr int kSpmvStages = 2;    // ring depth per warp

@@ -127,6 +127,7 @@ void validate_options(const pramaan_pdhg_options& opt) {
     if (opt.refine != 0 && opt.refine != 1) throw InvalidArgument("pdhg options: refine must be 0 or 1");
     if (opt.persistent < -1 || opt.persistent > 2) throw InvalidArgument("pdhg options: persistent must be -1, 0, 1 or 2");
     if (opt.gather_cache < -1 || opt.gather_cache > 1) throw InvalidArgument("pdhg options: gather_cache must be -1, 0 or 1");
+    if (opt.launch_blocks < 0 || opt.launch_blocks > 64) throw InvalidArgument("pdhg options: launch_blocks must be 0..64");
     if (opt.algorithm == PRAMAAN_ALGO_HALPERN && opt.refine != 1)
         throw InvalidArgument("pdhg options: the Halpern algorithm runs on FP64 master iterates (refine = 1)");
 }
@@ -224,16 +225,16 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
         const EpiPrimalRef pe{tau_.get(), c_.get(), lx_.get(), ux_.get(), xs.get(), xbs.get()};
         autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
             SpmvLauncher<EpiDualRef, float, float, false>::launch(v, xbar_.get(), de, status_.get(), st_, dev_);
-        }, /*kind=*/1);
+        }, /*kind=*/1, opt.launch_blocks);
         autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
             SpmvLauncher<EpiPrimalRef, float, float, false>::launch(v, y_.get(), pe, status_.get(), st_, dev_);
-        }, /*kind=*/2);
+        }, /*kind=*/2, opt.launch_blocks);
         PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // scratch copies are freed on return
     } else {
         // The FP32 product kernels share one shared-memory layout, so the grid the
         // tuner picks for the store-only kernel carries over to the adaptive epilogues.
-        autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache);
-        autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache);
+        autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache, {}, 0, opt.launch_blocks);
+        autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache, {}, 0, opt.launch_blocks);
     }
     if (adaptive_) {
         SpmvLauncher<EpiDualAdapt, float, float, false>::blocks_per_sm(dev_);

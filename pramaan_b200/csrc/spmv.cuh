@@ -42,14 +42,18 @@
 //
 // What bounds it
 //   On a random sparsity pattern every entry costs one 4-byte gather of x
-//   from L2, and B200 serves random gathers at about one L1 request per clock
-//   per SM (~288 G/s per GPU measured) whatever the cache operator, while
-//   the matrix stream itself needs well under half of HBM bandwidth at that
-//   rate (the Ax̄ product of a 108 M-entry power-law LP runs at 81 % of the
-//   L1TEX throughput).  Outstanding gather misses occupy L1 lines, so the
-//   kernel runs with a shared-memory carve-out sized for 3-4 blocks per SM
-//   (leaving ~100 KB of L1) rather than the largest carve-out: with the L1
-//   squeezed to ~40 KB the same kernel runs at half the gather rate.
+//   from L2, and B200 serves random gathers at about one sector request per
+//   clock per SM, whatever the cache operator: 279 G gathers/s measured by
+//   gather_ceiling_kernel (ceiling.cu), with the L1-to-crossbar request path
+//   97 % busy.  The matrix stream itself needs well under half of HBM
+//   bandwidth at that rate (the Ax̄ product of a 108 M-entry power-law LP runs
+//   at 0.84 of the gather rate).  Outstanding gather misses occupy L1 lines,
+//   so the plain kernel runs with a shared-memory carve-out sized for 3 blocks
+//   per SM (leaving ~100 KB of L1) rather than the largest carve-out: with the
+//   L1 squeezed to ~40 KB the same kernel runs at half the gather rate.  When
+//   the gathers are local (they hit L1) the product is latency-bound instead,
+//   and the dense variants (kStageAlias: finished rows staged over the tile's
+//   own slots, 4-5 blocks per SM) hide more of that latency.
 //
 // Schedule (spmv_warp_kernel)
 //   A persistent grid walks the tiles; every warp owns a private STAGES-deep
@@ -383,11 +387,16 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
         }
 
         // ---- walk my entries; stage the rows that end here ----
+        // Without branches: the first row end closes the head row when that
+        // row began before my first entry (head_bit); every other end stores
+        // its row into the staging buffer at row0 - base + (ends before it),
+        // a predicated store.  The sums are the same FMAs in the same order.
+        const uint32_t head_bit = head_before ? (ends & (0u - ends)) : 0u;
+        const bool head_pending = head_bit != 0u;
+        AccT* const fin_row = fin + (row0 - base);
         AccT acc = AccT(0);
-        int cur = row0;
-        int nemit = 0;
         AccT head_acc = AccT(0);
-        bool head_pending = false;
+        int k_end = 0;
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             if constexpr (kLo) {
@@ -395,14 +404,15 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
             } else {
                 acc = fma(static_cast<AccT>(vv[j]), static_cast<AccT>(xv[j]), acc);
             }
-            if ((ends >> j) & 1u) {
-                if (nemit == 0 && head_before) { head_acc = acc; head_pending = true; }
-                else fin[cur - base] = acc;
-                ++nemit;
-                ++cur;
-                acc = AccT(0);
-            }
+            const bool e = (ends >> j) & 1u;
+            const bool h = (head_bit >> j) & 1u;
+            if (e && !h) fin_row[k_end] = acc;
+            head_acc = h ? acc : head_acc;
+            k_end += e ? 1 : 0;
+            acc = e ? AccT(0) : acc;
         }
+        const int nemit = k_end;
+        const int cur = row0 + k_end;
 
         // ---- segmented warp scan of (row end seen, open partial) ----
         // Before the step of distance d, lane i's partial covers lanes

@@ -135,6 +135,7 @@ class PdhgOptions:
     gather_cache: int = 0       # 0: hot gather targets of large skewed operands in shared memory and
                                 # L1-cached gathers where the autotuner finds them faster;
                                 # 1: L1-cached gathers on every operand without hot slots; -1: plain
+    launch_blocks: int = 0      # 0: autotuned blocks per SM of the large-operand products; > 0: fixed
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -153,6 +154,7 @@ class PdhgOptions:
         o.refine = int(bool(self.refine))
         o.persistent = int(self.persistent)
         o.gather_cache = int(self.gather_cache)
+        o.launch_blocks = int(self.launch_blocks)
         return o
 
 

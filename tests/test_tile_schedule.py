@@ -375,3 +375,48 @@ def test_ballot_row_end_windows_equal_flag_shuffles():
             f = np.array([(f[i] | fo[i]) if i >= d else f[i] for i in range(32)])
             d <<= 1
         assert np.array_equal(v_old, v_new)
+
+
+def _stage_branchy(ends, head_before, row0, base, p):
+    """The per-entry row-end loop as first written: a branch per row end."""
+    fin, acc, cur, nemit, head_acc, head_pending = {}, 0, row0, 0, 0, False
+    for j in range(16):
+        acc += p[j]
+        if (ends >> j) & 1:
+            if nemit == 0 and head_before:
+                head_acc, head_pending = acc, True
+            else:
+                fin[cur - base] = acc
+            nemit += 1
+            cur += 1
+            acc = 0
+    return fin, acc, cur, nemit, head_acc, head_pending
+
+
+def _stage_branch_free(ends, head_before, row0, base, p):
+    """spmv_tiles' branch-free form: the first end closes the head row when
+    it began earlier; every other end stores at row0 - base + (ends before it)."""
+    head_bit = (ends & (-ends & 0xffffffff)) if head_before else 0
+    fin, acc, head_acc, k = {}, 0, 0, 0
+    for j in range(16):
+        acc += p[j]
+        e, h = (ends >> j) & 1, (head_bit >> j) & 1
+        if e and not h:
+            fin[row0 - base + k] = acc
+        head_acc = acc if h else head_acc
+        k += e
+        acc = 0 if e else acc
+    return fin, acc, row0 + k, k, head_acc, head_bit != 0
+
+
+def test_branch_free_row_end_staging_equals_the_branchy_loop():
+    rng = np.random.default_rng(11)
+    for _ in range(4000):
+        ends = int(rng.integers(0, 1 << 16))
+        if rng.random() < 0.2:
+            ends = 0
+        head_before = bool(rng.integers(0, 2))
+        row0 = int(rng.integers(0, 1000))
+        base = row0 - int(rng.integers(0, 3))
+        p = rng.integers(-9, 10, size=16)
+        assert _stage_branchy(ends, head_before, row0, base, p) == _stage_branch_free(ends, head_before, row0, base, p)
