@@ -74,6 +74,7 @@ def parse():
     p.add_argument("--stream-windows", type=int, default=4, help="windows per stream in that section")
     p.add_argument("--stream-T", type=int, nargs=2, default=(24, 336), help="periods of the stream windows")
     p.add_argument("--stream-P", type=int, nargs=2, default=(5, 50), help="products of the stream windows")
+    p.add_argument("--weights", default=None, help="warm-start network weights (.npz; default: the committed ones)")
     p.add_argument("--probe-iters", type=int, default=64,
                    help="PDHG iterations from each candidate start before the certificate chooses")
     p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
@@ -408,11 +409,12 @@ def learned_stream_section(args, device):
     from pramaan_b200.pdhg import ALGO_HALPERN
     from pramaan_b200.train_warm_start import DEFAULT_OUT, stream_windows
 
-    if not DEFAULT_OUT.exists():
-        return {"unavailable": f"no trained weights at {DEFAULT_OUT.name}"}
-    rec = json.loads(str(np.load(DEFAULT_OUT)["record"]))
+    wpath = Path(args.weights) if args.weights else DEFAULT_OUT
+    if not wpath.exists():
+        return {"unavailable": f"no trained weights at {wpath.name}"}
+    rec = json.loads(str(np.load(wpath)["record"]))
     net = WarmStartNet(device=device, seed=0)
-    net.load(DEFAULT_OUT)
+    net.load(wpath)
     tol = 1e-6
     o = PdhgOptions(tolerance=tol, max_iterations=400000, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=device)

@@ -196,7 +196,7 @@ def training_targets(results: list[SolveResult]) -> list[WarmStart]:
 @dataclass
 class WarmSolveInfo:
     warm_iterations: list[int]
-    choices: list[str]          # per LP: "network", "hint" or "cold" (the certified start)
+    choices: list[str]          # per LP: "network", "hint", "blend" or "cold" (the certified start)
     start_kkt: list[float]      # the chosen start's relative KKT error
     fallbacks: int
     predict_s: float
@@ -267,8 +267,9 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
     1. The network predicts (x, y, omega) for every LP (refining ``hints``
        when given, see ``GnnGraph``).
     2. The certificate decides the start of each LP: the network's point, the
-       hint or the cold start, whichever has the smallest FP64 relative KKT
-       error (``select_starts``), judged after ``probe_iterations`` PDHG
+       hint, (when probing) the point halfway between them, or the cold start,
+       whichever has the smallest FP64 relative KKT error (``select_starts``),
+       judged after ``probe_iterations`` PDHG
        iterations from each when that is > 0 (the solve then continues from
        the chosen probe's point; every probe's iterations are counted in
        ``WarmSolveInfo.probe_iterations``).
@@ -286,6 +287,12 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
     cands = {"network": pred}
     if hints is not None:
         cands["hint"] = list(hints)
+        # halfway between the hint and the network's refinement of it: the
+        # network's corrections are right on average, and often too large
+        if probe_iterations > 0:
+            cands["blend"] = [None if (h is None or p is None) else
+                              WarmStart(0.5 * (np.asarray(h.x) + p.x), 0.5 * (np.asarray(h.y) + p.y), 0.0)
+                              for h, p in zip(hints, pred)]
     starts, chosen, kkt, spent = select_starts(models, cands, net.device, probe_iterations, options)
     warm = []
     for st, nm, p in zip(starts, chosen, pred):

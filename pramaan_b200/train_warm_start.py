@@ -6,7 +6,7 @@ Usage:
 
 Generates S streams of W consecutive windows (rolling_horizon_stream: AR(1)
 demand, the window shifting by one period), labels every window with the
-batched restarted Halpern PDHG at 1e-6 relative KKT, builds each window's hint (the
+batched restarted Halpern PDHG (1e-6 relative KKT by default, ``--tol``), builds each window's hint (the
 previous window's solution shifted by one period; none for a stream's first
 window) and fits the network with Adam on mini-batches of 16 hinted windows.
 The labels are the PDHG's own solutions, so the network learns nothing the
@@ -69,9 +69,11 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--label-batch", type=int, default=1024)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--tol", type=float, default=1e-6, help="relative KKT of the PDHG labels")
+    ap.add_argument("--max-iterations", type=int, default=300000)
     ap.add_argument("--out", type=Path, default=DEFAULT_OUT)
     a = ap.parse_args(argv)
-    o = PdhgOptions(tolerance=1e-6, max_iterations=300000, check_frequency=64, algorithm=ALGO_HALPERN,
+    o = PdhgOptions(tolerance=a.tol, max_iterations=a.max_iterations, check_frequency=64, algorithm=ALGO_HALPERN,
                     device=a.device)
     t0 = time.time()
     models, first = stream_windows(range(a.seed0, a.seed0 + a.streams), a.windows, tuple(a.T), tuple(a.P))
@@ -94,7 +96,7 @@ def main(argv=None):
     record = {"instances_solved": len(models), "instances_trained": len(idx), "streams": a.streams,
               "windows": a.windows, "T": list(a.T), "P": list(a.P), "epochs": a.epochs, "lr": a.lr,
               "label_s": t_label, "train_s": t_train, "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
-              "optimal_labels": sum(r.status == SolveStatus.kOptimal for r in results)}
+              "optimal_labels": sum(r.status == SolveStatus.kOptimal for r in results), "label_tol": a.tol}
     a.out.parent.mkdir(parents=True, exist_ok=True)
     np.savez(a.out, params=net.params, record=json.dumps(record))
     print(json.dumps(record))

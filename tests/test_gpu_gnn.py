@@ -241,3 +241,39 @@ def test_learned_warm_start_saves_iterations_on_a_stream():
     cert = certify_batch(ev, [[WarmStart(r.x, r.y) for r in res]])[0]
     for r, c in zip(res, cert):
         assert r.status == SolveStatus.kOptimal and c.kkt <= 1e-6 * 1.0001
+
+
+def test_learned_start_measured_against_the_hint_it_refines():
+    """What the trained network adds over the method without it.  The method
+    without it starts each window from the previous window's shifted solution
+    (the hint).  The certified learned pipeline lets the FP64 certificate
+    choose, after a 64-iteration probe from each candidate, between the
+    network's refinement of the hint, the hint, their midpoint and the cold
+    start.  On held-out streams both are measured in total PDHG iterations,
+    the learned pipeline's probes included.  The network's refinement is not
+    a reliable gain over the hint it refines (on the benchmark stream it
+    needs 5 % more iterations), so what is asserted is that the
+    certified pipeline never falls far behind the hint, that both beat cold
+    starts, and that every answer is certified."""
+    from pramaan_b200.certificate import certify_batch
+    from pramaan_b200.train_warm_start import DEFAULT_OUT
+    o = opts()
+    ev, fev = _stream_set(range(3950, 3956), 6, (24, 96), (5, 20))
+    cold = solve_batch(ev, o)
+    assert all(r.status == SolveStatus.kOptimal for r in cold)
+    hev = _hints(ev, fev, cold)
+    net = WarmStartNet(seed=0)
+    net.load(DEFAULT_OUT)
+    hint = solve_batch(ev, o, warm=hev)
+    res, info = warm_solve_batch(ev, net, o, hints=hev, probe_iterations=64)
+    cold_total = sum(r.iterations for r in cold)
+    hint_total = sum(r.iterations for r in hint)
+    learned_total = sum(info.warm_iterations) + info.probe_iterations
+    print(f"iterations: cold {cold_total}, hint {hint_total} ({hint_total / cold_total:.3f}), learned "
+          f"{learned_total} ({learned_total / cold_total:.3f}, {learned_total / hint_total:.3f} of hint); "
+          f"starts {dict((c, info.choices.count(c)) for c in set(info.choices))}")
+    assert hint_total < cold_total and learned_total < cold_total
+    assert learned_total <= 1.15 * hint_total
+    cert = certify_batch(ev, [[WarmStart(r.x, r.y) for r in res]])[0]
+    for r, c in zip(res, cert):
+        assert r.status == SolveStatus.kOptimal and c.kkt <= 1e-6 * 1.0001
