@@ -70,6 +70,8 @@ def parse():
     p.add_argument("--solver-cap-s", type=float, default=20.0,
                    help="wall-clock cap of one reference CPU solve at full size (reported as DNF)")
     p.add_argument("--rh-plain", type=int, default=8, help="LPs of that batch also solved one by one")
+    p.add_argument("--batch-iters", type=int, default=256,
+                   help="iterations of the batched-products timing (every LP active)")
     p.add_argument("--stream-count", type=int, default=32, help="streams of the learned warm-start section")
     p.add_argument("--stream-windows", type=int, default=4, help="windows per stream in that section")
     p.add_argument("--stream-T", type=int, nargs=2, default=(24, 336), help="periods of the stream windows")
@@ -83,7 +85,7 @@ def parse():
     p.add_argument("--launch-blocks", type=int, default=0,
                    help="fixed blocks per SM of the products (0: autotuned); with --gather-cache 1 or -1 "
                         "the launch shape is fixed, for profiles")
-    p.add_argument("--only", default=None, choices=["banded", "gnn", "small", "rolling", "stream", "ceiling", "ladder", "solvers"],
+    p.add_argument("--only", default=None, choices=["banded", "gnn", "small", "rolling", "stream", "ceiling", "ladder", "solvers", "batch"],
                    help="run one section alone on the given sizes and print its JSON (profiling runs)")
     p.add_argument("--gnn-lps", type=int, default=64, help="rolling-horizon LPs of the network throughput section")
     p.add_argument("--gnn-reps", type=int, default=5)
@@ -397,6 +399,42 @@ def rolling_horizon_section(args, device, dist=None):
             "plain_time_to_tol_median_s": float(np.median(plain_t)),
             "plain_iterations_median": float(np.median(plain_it)),
             "batched_over_plain": batched / plain}
+
+
+def batch_iteration_section(args, device, models=None):
+    """The batched products' own speed: the rolling-horizon batch run for a
+    fixed number of iterations with every LP active (tolerance 0), timed as
+    the difference of a 2K- and a K-iteration solve so that set-up cancels.
+    Algorithmic bytes per iteration over the packed operand: the matrix
+    streams and gathers of both products (16 nnz + 8 (m + n)) plus the
+    Halpern epilogues' vectors (primal: tau, c, bounds, x, LP index read,
+    x and x-bar written, 32 B per column; dual: sigma, bounds, master y,
+    y, LP index read, y written, 28 B per row)."""
+    from pramaan_b200 import PdhgOptions, solve_batch
+    from pramaan_b200.generators import rolling_horizon_batch
+    from pramaan_b200.pdhg import ALGO_HALPERN
+
+    if models is None:
+        models = rolling_horizon_batch(args.rh_count, seed=args.seed)
+    K = args.batch_iters
+    times = {}
+    for k in (K, 2 * K):
+        o = PdhgOptions(tolerance=0.0, max_iterations=k, check_frequency=64, algorithm=ALGO_HALPERN, device=device)
+        if k == K:
+            solve_batch(models[:2], o)   # warm-up
+        t0 = time.perf_counter()
+        solve_batch(models, o)
+        times[k] = time.perf_counter() - t0
+    per_it = (times[2 * K] - times[K]) / K
+    m = sum(md.numRows() for md in models)
+    n = sum(md.numVars() for md in models)
+    nnz = sum(md.nnz() for md in models)
+    by = 16.0 * nnz + 8.0 * (m + n) + 32.0 * n + 28.0 * m
+    hbm, kind = measured_peaks()
+    return {"workload": f"rolling_horizon_batch {len(models)} LPs, every LP active, {K} vs {2 * K} iterations",
+            "rows": m, "cols": n, "nnz": nnz, "us_per_iteration": per_it * 1e6,
+            "algorithmic_bytes_per_iteration": by, "achieved_gbs": by / per_it / 1e9, "frac": by / per_it / 1e9 / hbm,
+            "peak_gbs": hbm, "peak_kind": kind}
 
 
 def learned_stream_section(args, device):
@@ -732,6 +770,7 @@ def run_gpu_arm(args):
                     "stream": learned_stream_section,
                     "ceiling": lambda a, d: gather_ceiling(a.n, d),
                     "ladder": ladder_section, "solvers": reference_solvers_section,
+                    "batch": batch_iteration_section,
                     "rolling": lambda a, d: rolling_horizon_section(a, d, dist)}
         out = sections[args.only](args, local)
         if rank == 0:
@@ -873,6 +912,8 @@ def run_gpu_arm(args):
         line["ladder_lp"] = ladder_section(args, local)
     if not args.no_rolling:
         line["rolling_horizon"] = rolling_horizon_section(args, local, dist)
+    if single and not args.no_rolling:
+        line["batched_products"] = batch_iteration_section(args, local)
     if single and not args.no_rolling:
         line["learned_stream"] = learned_stream_section(args, local)
         line["gnn_throughput"] = gnn_section(args, local)
