@@ -170,26 +170,38 @@ struct EpiPrimalHalpern {
         prefetch_l2(tau + j); prefetch_l2(c + j); prefetch_l2(l_x + j); prefetch_l2(u_x + j);
         prefetch_l2(x + j); if (lp) prefetch_l2(lp + j);
     }
-    __device__ void apply(State&, int j, float aty) const {
-        const float x_prev = x[j];
-        const float t = tau[j];
-        if (!(t > 0.0f)) {           // a frozen LP keeps its iterate
-            x_bar[j] = x_prev;
+    // apply() split in two: every input of column j, then the update
+    // (the tile loop loads several columns ahead of their updates).
+    static constexpr bool kSplit = true;
+    struct In { float x_prev, t, c, lo, hi, a, w; };
+    __device__ In load(int j) const {
+        In in;
+        in.x_prev = x[j];
+        in.t = tau[j];
+        in.c = c[j];
+        in.lo = l_x[j];
+        in.hi = u_x[j];
+        in.a = anchor ? anchor[j] : 0.0f;
+        in.w = halpern_weight(iter_base, offset, restart_iter, lp, j);
+        return in;
+    }
+    __device__ void store(State&, int j, const In& in, float aty) const {
+        if (!(in.t > 0.0f)) {        // a frozen LP keeps its iterate
+            x_bar[j] = in.x_prev;
             if (fpr) fpr[j] = 0.0;
             return;
         }
-        const float g = __fadd_rn(c[j], aty);
-        const float xt = fminf(fmaxf(__fmaf_rn(-t, g, x_prev), l_x[j]), u_x[j]);
-        x_bar[j] = __fmaf_rn(2.0f, xt, -x_prev);
-        const float w = halpern_weight(iter_base, offset, restart_iter, lp, j);
-        const float refl = __fmaf_rn(1.0f + kHalpernReflection, xt, -kHalpernReflection * x_prev);
-        const float a = anchor ? anchor[j] : 0.0f;
-        x[j] = __fmaf_rn(w, __fsub_rn(refl, a), a);
+        const float g = __fadd_rn(in.c, aty);
+        const float xt = fminf(fmaxf(__fmaf_rn(-in.t, g, in.x_prev), in.lo), in.hi);
+        x_bar[j] = __fmaf_rn(2.0f, xt, -in.x_prev);
+        const float refl = __fmaf_rn(1.0f + kHalpernReflection, xt, -kHalpernReflection * in.x_prev);
+        x[j] = __fmaf_rn(in.w, __fsub_rn(refl, in.a), in.a);
         if (fpr) {
-            const double d = double(x_prev) - double(xt);
-            fpr[j] = d * d / double(t);
+            const double d = double(in.x_prev) - double(xt);
+            fpr[j] = d * d / double(in.t);
         }
     }
+    __device__ void apply(State& st, int j, float aty) const { store(st, j, load(j), aty); }
     __device__ void finish(State&, int) const {}
 };
 
@@ -211,28 +223,40 @@ struct EpiDualHalpern {
         prefetch_l2(sigma + i); prefetch_l2(r_lo + i); prefetch_l2(r_hi + i); prefetch_l2(y_m + i);
         prefetch_l2(e + i); if (lp) prefetch_l2(lp + i);
     }
-    __device__ void apply(State&, int i, float ad) const {
-        const float s = sigma[i];
-        const float e_prev = e[i];
+    static constexpr bool kSplit = true;
+    struct In { float s, e_prev, ym, hi, lo, a, w; };
+    __device__ In load(int i) const {
+        In in;
+        in.s = sigma[i];
+        in.e_prev = e[i];
+        in.ym = y_m[i];
+        in.hi = r_hi[i];
+        in.lo = r_lo[i];
+        in.a = anchor ? anchor[i] : 0.0f;
+        in.w = halpern_weight(iter_base, offset, restart_iter, lp, i);
+        return in;
+    }
+    __device__ void store(State&, int i, const In& in, float ad) const {
+        const float s = in.s;
+        const float e_prev = in.e_prev;
         float en = e_prev;
         if (s > 0.0f) {
-            const float ym = y_m[i];
+            const float ym = in.ym;
             const float q = __fdiv_rn(__fadd_rn(ym, e_prev), s);
-            const float hi = __fadd_rn(ad, r_hi[i]);
-            const float lo = __fadd_rn(ad, r_lo[i]);
+            const float hi = __fadd_rn(ad, in.hi);
+            const float lo = __fadd_rn(ad, in.lo);
             if (__fadd_rn(q, hi) > 0.0f) en = __fmaf_rn(s, hi, e_prev);
             else if (__fadd_rn(q, lo) < 0.0f) en = __fmaf_rn(s, lo, e_prev);
             else en = -ym;
         }
-        const float w = halpern_weight(iter_base, offset, restart_iter, lp, i);
         const float refl = __fmaf_rn(1.0f + kHalpernReflection, en, -kHalpernReflection * e_prev);
-        const float a = anchor ? anchor[i] : 0.0f;
-        e[i] = __fmaf_rn(w, __fsub_rn(refl, a), a);
+        e[i] = __fmaf_rn(in.w, __fsub_rn(refl, in.a), in.a);
         if (fpr) {
             const double d = double(e_prev) - double(en);
             fpr[i] = s > 0.0f ? d * d / double(s) : 0.0;
         }
     }
+    __device__ void apply(State& st, int i, float ad) const { store(st, i, load(i), ad); }
     __device__ void finish(State&, int) const {}
 };
 

@@ -531,8 +531,6 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     warm_launcher<EpiStore<double, double>, double, double>(dev_);
     warm_launcher<EpiRowViolOut, double, double>(dev_);
     warm_launcher<EpiColResidOut, double, double>(dev_);
-    autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
-    autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
     estimate_step_sizes();
 
     // initial primal weight per LP: ||C c|| / ||R b|| on the scaled LP
@@ -558,6 +556,11 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
         }
     }
     apply_steps();
+    if (halpern_) {
+        set_int_kernel<<<1, 1, 0, st_>>>(iter_base_.get(), 0);
+        PB_CUDA_CHECK(cudaGetLastError());
+    }
+    tune_products();
     if (cluster_ok_) build_cluster_lps();
     PB_CUDA_CHECK(cudaStreamSynchronize(st_));
     // the packed host CSR stays for compaction
@@ -1383,8 +1386,6 @@ void AdaptiveBatch::compact() {
         nA.keep_flat = nAT.keep_flat = cluster_ok_;
         nA.pack(st_);
         nAT.pack(st_);
-        autotune_operand(nA, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
-        autotune_operand(nAT, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
     }
 
     // 4. the first compaction keeps the original layout for the final evaluation
@@ -1433,7 +1434,41 @@ void AdaptiveBatch::compact() {
     graph_iters_ = 0;
     compacted_ = true;
     ++compactions_;
+    tune_products();
     if (cluster_ok_) build_cluster_lps();
+}
+
+// The launch autotuner on the current operands.  In Halpern mode it times the
+// products the iteration runs (EpiPrimalHalpern / EpiDualHalpern, writing
+// scratch copies of x, x̄ and y): on the rolling-horizon batches most rows
+// hold two or three entries, so the epilogue's loads, which a store-only
+// proxy does not have, set the best number of resident blocks.
+void AdaptiveBatch::tune_products() {
+    if (!halpern_) {
+        autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
+        autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
+        return;
+    }
+    DevBuf<float> xs(size_t(n_ > 0 ? n_ : 1)), xbs(size_t(n_ > 0 ? n_ : 1)), es(size_t(m_ > 0 ? m_ : 1));
+    if (n_ > 0) {
+        PB_CUDA_CHECK(cudaMemcpyAsync(xs.get(), x_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
+        PB_CUDA_CHECK(cudaMemcpyAsync(xbs.get(), xbar_.get(), size_t(n_) * 4, cudaMemcpyDeviceToDevice, st_));
+    }
+    if (m_ > 0) PB_CUDA_CHECK(cudaMemcpyAsync(es.get(), y_.get(), size_t(m_) * 4, cudaMemcpyDeviceToDevice, st_));
+    const int* lpc = K_ == 1 ? nullptr : lp_col_.get();
+    const int* lpr = K_ == 1 ? nullptr : lp_row_.get();
+    const EpiPrimalHalpern ep{tau_.get(), c_.get(), lx_.get(), ux_.get(), xs.get(), xbs.get(), nullptr, lpc,
+                              restart_iter_.get(), iter_base_.get(), 0, nullptr};
+    const EpiDualHalpern ed{sigma_.get(), lr_.get(), ur_.get(), ym32_.get(), es.get(), nullptr, lpr,
+                            restart_iter_.get(), iter_base_.get(), 0, nullptr};
+    autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache, [&](const CsrView& v) {
+        SpmvLauncher<EpiPrimalHalpern, float, float, false>::launch(v, y_.get(), ep, status_.get(), st_, dev_);
+    }, /*kind=*/3, opt_.launch_blocks);
+    if (m_ > 0)
+        autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache, [&](const CsrView& v) {
+            SpmvLauncher<EpiDualHalpern, float, float, false>::launch(v, xbar_.get(), ed, status_.get(), st_, dev_);
+        }, /*kind=*/4, opt_.launch_blocks);
+    PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // scratch copies are freed on return
 }
 
 void AdaptiveBatch::finish(const pramaan_lp* lps, pramaan_solve_result* results, double solve_ms) {

@@ -111,6 +111,8 @@ private:
     void check_status();
     // Rebuilds the operand from the LPs still iterating (see above).
     void compact();
+    // Launch shapes of the current operands (the products the iteration runs).
+    void tune_products();
     // x_out / y_out (original layout) = master + correction of the LPs in the
     // current operand whose keep flag is 0 (all of them when keep is null).
     void scatter_answers(const int* keep);

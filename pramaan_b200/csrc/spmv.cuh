@@ -208,6 +208,15 @@ struct SpmvSmemLayout {
 //                                                          // (channel 0: main kernel, 1: fixup)
 //   };
 
+// Epilogues that split apply() into load(row) -> In and store(State&, row,
+// In, value) declare `static constexpr bool kSplit = true`; the tile loop
+// then loads kEpiPass rows per lane ahead of their updates.
+template <class Epi, class = void>
+struct EpiSplit { static constexpr bool value = false; };
+template <class Epi>
+struct EpiSplit<Epi, decltype(void(Epi::kSplit))> { static constexpr bool value = Epi::kSplit; };
+constexpr int kEpiPass = 4;
+
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
@@ -442,9 +451,30 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
         __syncwarp();
 
         // ---- epilogue over the finished rows, one row per lane (coalesced) ----
-        for (int k = lane; k < n_fin; k += 32) {
-            const int rc = base + k;
-            epi.apply(est, kRowMap ? A.row_map[rc] : rc, fin[k]);
+        if constexpr (EpiSplit<Epi>::value) {
+            // Epilogues with a separate load step: the inputs of kEpiPass rows
+            // per lane are loaded before any of them is updated, so the loads
+            // of a tile with many short rows overlap instead of running one
+            // round trip per 32 rows.
+            constexpr int U = kEpiPass;
+            for (int k0 = lane; k0 < n_fin; k0 += 32 * U) {
+                typename Epi::In in[U];
+                int row[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = k0 + 32 * u;
+                    row[u] = k < n_fin ? (kRowMap ? A.row_map[base + k] : base + k) : -1;
+                    if (row[u] >= 0) in[u] = epi.load(row[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (row[u] >= 0) epi.store(est, row[u], in[u], fin[k0 + 32 * u]);
+            }
+        } else {
+            for (int k = lane; k < n_fin; k += 32) {
+                const int rc = base + k;
+                epi.apply(est, kRowMap ? A.row_map[rc] : rc, fin[k]);
+            }
         }
         __syncwarp();   // stage s and the staged values are free for reuse
         if (lane == 0 && i + STAGES < mine) {
