@@ -70,7 +70,7 @@ def parse():
     p.add_argument("--solver-cap-s", type=float, default=20.0,
                    help="wall-clock cap of one reference CPU solve at full size (reported as DNF)")
     p.add_argument("--rh-plain", type=int, default=8, help="LPs of that batch also solved one by one")
-    p.add_argument("--batch-iters", type=int, default=256,
+    p.add_argument("--batch-iters", type=int, default=1024,
                    help="iterations of the batched-products timing (every LP active)")
     p.add_argument("--stream-count", type=int, default=32, help="streams of the learned warm-start section")
     p.add_argument("--stream-windows", type=int, default=4, help="windows per stream in that section")
