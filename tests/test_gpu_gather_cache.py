@@ -139,3 +139,28 @@ def test_hot_slots_with_row_maps_identical(zipf_mid):
         assert runs[cache][1] == runs[-1][1]
     # the emptied columns keep their clamped start; the emptied rows move only with their bounds
     assert np.isfinite(runs[0][2]).all()
+
+
+@pytest.mark.parametrize("blocks", [1, 3, 5])
+def test_launch_shape_changes_no_iterate(blocks):
+    """The launch shape (`launch_blocks`: resident blocks per SM; above 3 the
+    dense variants, which stage finished rows over the tile's own slots)
+    only moves tiles between warps: every tile is summed by the same code and
+    rows crossing tiles are completed in tile order.  On a banded LP large
+    enough for the autotuner, the iterates after 40 reference iterations, the
+    FP64 residuals and a Halpern solve are bit-identical to the autotuned
+    launch's, with L1-cached and with L2 gathers."""
+    md = gen.banded_lp(200_000, 500_000, per_row=24, band=128, seed=5)
+    for cache in (1, -1):
+        runs = []
+        for lb in (0, blocks):
+            o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+                            gather_cache=cache, launch_blocks=lb)
+            with Session(md, o) as s:
+                s.iterate(40)
+                runs.append((s.residuals(), *s.iterates()))
+        (r0, x0, y0), (r1, x1, y1) = runs
+        assert np.array_equal(x0, x1) and np.array_equal(y0, y1) and r0 == r1
+    h = [PdhgSolver(PdhgOptions(tolerance=1e-12, max_iterations=256, check_frequency=64, algorithm=ALGO_HALPERN,
+                                launch_blocks=lb)).solve(md) for lb in (0, blocks)]
+    assert h[0].iterations == h[1].iterations and np.array_equal(h[0].x, h[1].x)
