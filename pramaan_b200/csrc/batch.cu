@@ -829,6 +829,10 @@ void AdaptiveBatch::launch_interval(int k) {
 // cluster kernel was 4x slower than the packed tiled products, whose grid
 // spreads every LP over the whole GPU.
 constexpr long long kClusterAutoMaxNnz = 1LL << 20;
+// Halpern mode compacts the operand once the LPs still iterating hold less
+// than this share of its non-zeros (a compaction costs ~0.1 s on the 512-LP
+// batch; the frozen LPs' share of every product before it is pure waste).
+constexpr double kCompactLiveShare = 0.75;
 constexpr int kClusterAutoMin = 16;
 
 void AdaptiveBatch::build_cluster_lps() {
@@ -1315,7 +1319,9 @@ void AdaptiveBatch::solve_halpern() {
         const bool to_cluster = cluster_ok_ && opt_.persistent == 0 && !use_cluster_kernel() && live_lps > 0 &&
                                 live_lps < cluster_nlps_ &&
                                 (long long)live_lps * kClusterAutoMin <= device_sm_count(dev_);
-        if (live > 0 && ((2 * live < (long long)nnz_ && (long long)nnz_ - live >= 65536) || to_cluster)) compact();
+        if (live > 0 && ((double(live) < kCompactLiveShare * double(nnz_) && (long long)nnz_ - live >= 65536) ||
+                         to_cluster))
+            compact();
     }
     for (Lp& s : lp_)
         if (s.status == PRAMAAN_STATUS_ITERATION_LIMIT) s.iterations = max_it;
@@ -1444,6 +1450,8 @@ void AdaptiveBatch::compact() {
 // hold two or three entries, so the epilogue's loads, which a store-only
 // proxy does not have, set the best number of resident blocks.
 void AdaptiveBatch::tune_products() {
+    // the iteration's vectors: steps, bounds, master and correction iterates, LP indices
+    mark_l2_resident(A_, AT_, 32.0 * m_ + 36.0 * n_, dev_);
     if (!halpern_) {
         autotune_operand(A_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);
         autotune_operand(AT_, st_, dev_, status_.get(), opt_.gather_cache, {}, 0, opt_.launch_blocks);

@@ -16,8 +16,8 @@
 //     order), so a batch is deterministic run to run;
 //   * restarts, omega updates and the FP64 refinement folds act on the LPs
 //     that asked for them (an action code per LP);
-//   * when the LPs still iterating hold less than half of the operand's
-//     non-zeros, the operand is rebuilt from them alone and every per-row /
+//   * when the LPs still iterating hold less than half (Halpern mode: three
+//     quarters) of the operand's non-zeros, the operand is rebuilt from them alone and every per-row /
 //     per-column array is gathered into the new layout (converged LPs leave
 //     their answers in full-layout output arrays first), so the cost of an
 //     iteration follows the work that is left.

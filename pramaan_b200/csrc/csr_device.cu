@@ -574,6 +574,15 @@ void csr_upload_f32(CsrDevice& A, int rows, int cols, int nnz, const int* h_row_
     A.finalize(st);
 }
 
+void mark_l2_resident(CsrDevice& A, CsrDevice& AT, double vector_bytes, int dev) {
+    int l2 = 0;
+    PB_CUDA_CHECK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+    const double need = double(A.rec.bytes()) + double(AT.rec.bytes()) + vector_bytes;
+    const int keep = (l2 > 0 && need <= kL2ResidentShare * double(l2)) ? 1 : 0;
+    A.l2_resident = keep;
+    AT.l2_resident = keep;
+}
+
 void csr_transpose(const CsrDevice& A, CsrDevice& AT, cudaStream_t st) {
     const int nnz = A.nnz;
     AT.allocate(A.cols, A.rows, nnz, A.has_lo);

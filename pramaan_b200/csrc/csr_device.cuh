@@ -96,6 +96,7 @@ public:
     int tuned_blocks_per_sm = 0;   // set by the launch autotuner (0: default)
     int hot = 0;                   // hot gather slots
     int gather_l1 = 0;             // gathers cached in L1 (set by the launch autotuner)
+    int l2_resident = 0;           // keep the records in L2 between launches (see mark_l2_resident)
     bool has_lo = false;
     bool packed = false;
     bool keep_flat = false;        // pack() keeps the flat col / val (FP32) arrays
@@ -119,6 +120,7 @@ public:
         v.cross = cross.get(); v.carry = carry.get();
         v.hot = hot; v.hot_idx = hot_idx.get();
         v.gather_l1 = gather_l1;
+        v.l2_resident = l2_resident;
         return v;
     }
 
@@ -170,6 +172,14 @@ void select_hot_pair(CsrDevice& A, CsrDevice& AT, int dev, cudaStream_t st);
 // Launch helpers
 // ---------------------------------------------------------------------------
 int device_sm_count(int dev);
+
+// Marks the two operands of an iteration L2-resident when their tile records
+// and `vector_bytes` of per-iteration vectors fit in kL2ResidentShare of the
+// device's L2: their bulk copies then load with an evict-last policy, so the
+// next product reads them from L2 instead of HBM.  Larger operands keep the
+// evict-first policy (streamed once per product).
+constexpr double kL2ResidentShare = 0.85;
+void mark_l2_resident(CsrDevice& A, CsrDevice& AT, double vector_bytes, int dev);
 
 // Launch autotuner (results remembered per device, operand signature and
 // timed product: shape, crossing and empty rows, hot slots, option, `kind`):

@@ -203,6 +203,8 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     if (opt.gather_cache >= 0) select_hot_pair(A_, AT_, dev_, st_);
     A_.pack(st_);
     AT_.pack(st_);
+    // the iteration's vectors: sigma, bounds, y (rows); tau, c, bounds, x, x̄ (columns), plus the gathers
+    mark_l2_resident(A_, AT_, 20.0 * m_ + 28.0 * n_, dev_);
     // Occupancy queries / smem attributes before any graph capture.
     SpmvLauncher<EpiDualRef, float, float, false>::blocks_per_sm(dev_);
     SpmvLauncher<EpiPrimalRef, float, float, false>::blocks_per_sm(dev_);

@@ -129,6 +129,7 @@ struct CsrView {
     int hot = 0;                      // hot gather slots (records hold ~slot for them)
     const int* hot_idx = nullptr;     // hot: gather target of every slot
     int gather_l1 = 0;                // gathers cached in L1 (operands without hot slots)
+    int l2_resident = 0;              // records fit in L2 with the iteration's vectors: keep them
 };
 
 // Gather modes of the product kernel.
@@ -271,7 +272,9 @@ __device__ __forceinline__ bool spmv_tiles(const CsrView& A, const XT* __restric
             for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
             fence_mbar_init();
         }
-        policy = l2_policy_evict_first();
+        // Records of an operand that fits in L2 (with the other operand and the
+        // vectors) stay there for the next launch; the others stream through.
+        policy = A.l2_resident ? l2_policy_evict_last() : l2_policy_evict_first();
     }
     __syncwarp();
 
