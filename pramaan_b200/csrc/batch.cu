@@ -387,7 +387,7 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     m_ = int(m); n_ = int(n); nnz_ = int(nnz);
     full_m_ = m_; full_n_ = n_;
     PB_CUDA_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    PB_CUDA_CHECK(cudaMallocHost(&h_status_, sizeof(int)));
+    PB_CUDA_CHECK(pinned_alloc(&h_status_, sizeof(int)));
     status_.alloc(1);
     PB_CUDA_CHECK(cudaMemsetAsync(status_.get(), 0, sizeof(int), st_));
     if (K_ == 0) return;
@@ -455,13 +455,13 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
         }
     }
 
-    PB_CUDA_CHECK(cudaMallocHost(&h_action_, sizeof(int) * K_));
-    PB_CUDA_CHECK(cudaMallocHost(&h_inv_, sizeof(double) * K_));
-    PB_CUDA_CHECK(cudaMallocHost(&h_dscale_, sizeof(float) * K_));
-    PB_CUDA_CHECK(cudaMallocHost(&h_pscale_, sizeof(float) * K_));
-    PB_CUDA_CHECK(cudaMallocHost(&h_lp_f_, sizeof(float) * K_));
-    PB_CUDA_CHECK(cudaMallocHost(&h_out_, sizeof(double) * K_ * kOutWidth));
-    PB_CUDA_CHECK(cudaMallocHost(&h_keep_, sizeof(int) * K_));
+    PB_CUDA_CHECK(pinned_alloc(&h_action_, sizeof(int) * K_));
+    PB_CUDA_CHECK(pinned_alloc(&h_inv_, sizeof(double) * K_));
+    PB_CUDA_CHECK(pinned_alloc(&h_dscale_, sizeof(float) * K_));
+    PB_CUDA_CHECK(pinned_alloc(&h_pscale_, sizeof(float) * K_));
+    PB_CUDA_CHECK(pinned_alloc(&h_lp_f_, sizeof(float) * K_));
+    PB_CUDA_CHECK(pinned_alloc(&h_out_, sizeof(double) * K_ * kOutWidth));
+    PB_CUDA_CHECK(pinned_alloc(&h_keep_, sizeof(int) * K_));
 
     // ---- matrix: upload + validate, hi/lo split, transpose ----
     {
@@ -498,7 +498,7 @@ AdaptiveBatch::AdaptiveBatch(const pramaan_lp* lps, int count, const pramaan_pdh
     if (halpern_) {
         restart_iter_.alloc(K_);
         iter_base_.alloc(1);
-        PB_CUDA_CHECK(cudaMallocHost(&h_restart_iter_, sizeof(int) * K_));
+        PB_CUDA_CHECK(pinned_alloc(&h_restart_iter_, sizeof(int) * K_));
         for (int q = 0; q < K_; ++q) h_restart_iter_[q] = 0;
         PB_CUDA_CHECK(cudaMemcpyAsync(restart_iter_.get(), h_restart_iter_, sizeof(int) * K_, cudaMemcpyHostToDevice, st_));
         for (int b = 0; b < 2; ++b) {
@@ -573,6 +573,7 @@ AdaptiveBatch::~AdaptiveBatch() {
     if (st_) cudaStreamSynchronize(st_);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (graph_) cudaGraphDestroy(graph_);
+    DeviceSyncScope gate;
     if (h_action_) cudaFreeHost(h_action_);
     if (h_restart_iter_) cudaFreeHost(h_restart_iter_);
     if (h_inv_) cudaFreeHost(h_inv_);
@@ -927,16 +928,19 @@ void AdaptiveBatch::iterate(int k, int iter) {
         if (graph_iters_ != k) {
             if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
             if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
-            PB_CUDA_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-            try {
-                for (int i = 0; i < k; ++i) iterate_once(i, k);
-            } catch (...) {
-                cudaGraph_t g = nullptr;
-                cudaStreamEndCapture(st_, &g);
-                if (g) cudaGraphDestroy(g);
-                throw;
+            {
+                CaptureScope capture;
+                PB_CUDA_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+                try {
+                    for (int i = 0; i < k; ++i) iterate_once(i, k);
+                } catch (...) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(st_, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                PB_CUDA_CHECK(cudaStreamEndCapture(st_, &graph_));
             }
-            PB_CUDA_CHECK(cudaStreamEndCapture(st_, &graph_));
             PB_CUDA_CHECK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
             graph_iters_ = k;
         }

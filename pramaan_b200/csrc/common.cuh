@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
+#include <shared_mutex>
 #include <stdexcept>
 #include <string>
 
@@ -36,6 +38,39 @@ struct InvalidArgument : std::invalid_argument {
 struct DeviceTimeout : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+
+// Graph captures run in thread-local mode, which still breaks when another
+// host thread makes a call that synchronises with every stream of the device
+// (cudaDeviceSynchronize, cudaFree, cudaFreeHost, cudaMallocHost) while the
+// capture is open.  Each capture holds this gate shared from begin to end and
+// each such call holds it exclusively, so solves running concurrently from
+// several host threads stay legal.
+inline std::shared_mutex& capture_gate() {
+    static std::shared_mutex m;
+    return m;
+}
+inline bool& capture_open_here() {
+    thread_local bool open = false;
+    return open;
+}
+struct CaptureScope {
+    std::shared_lock<std::shared_mutex> lk{capture_gate()};
+    CaptureScope() { capture_open_here() = true; }
+    ~CaptureScope() { capture_open_here() = false; }
+};
+// A thread whose own capture is open never takes the gate exclusively (it
+// would wait on itself); CUDA rejects the call in that thread instead.
+struct DeviceSyncScope {
+    std::unique_lock<std::shared_mutex> lk;
+    DeviceSyncScope() {
+        if (!capture_open_here()) lk = std::unique_lock<std::shared_mutex>(capture_gate());
+    }
+};
+template <class T>
+cudaError_t pinned_alloc(T** p, size_t bytes) {
+    DeviceSyncScope gate;
+    return cudaMallocHost(reinterpret_cast<void**>(p), bytes);
+}
 
 // Device status word bits (written by kernels, read by the host after a sync).
 enum : int {

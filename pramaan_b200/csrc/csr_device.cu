@@ -314,6 +314,7 @@ void device_cache_free(void* p) noexcept {
     if (cur != b.dev) (void)cudaSetDevice(b.dev);
     // cudaFree waits for the device; a cached block must not be reused while
     // work issued before its release may still read or write it
+    DeviceSyncScope gate;
     const cudaError_t e = cudaDeviceSynchronize();
     bool keep = e == cudaSuccess;
     if (keep) {
@@ -343,6 +344,7 @@ void device_cache_release(int dev) {
     }
     int cur = -1;
     (void)cudaGetDevice(&cur);
+    DeviceSyncScope gate;
     for (auto& [d, p] : out) {
         if (d != cur) (void)cudaSetDevice(d);
         (void)cudaFree(p);

@@ -145,7 +145,7 @@ void PdhgEngine::setup_adaptive(const pramaan_lp& lp) {
     scal_.alloc(2);
     part_.alloc(size_t(kPartRows) * kPartSlots);
     red_.alloc(kPartSlots);
-    PB_CUDA_CHECK(cudaMallocHost(&h_red_, sizeof(double) * kPartSlots));
+    PB_CUDA_CHECK(pinned_alloc(&h_red_, sizeof(double) * kPartSlots));
     if (n_) PB_CUDA_CHECK(cudaMemsetAsync(xsum_.get(), 0, xsum_.bytes(), st_));
     if (m_) PB_CUDA_CHECK(cudaMemsetAsync(ysum_.get(), 0, ysum_.bytes(), st_));
     preconditioned_steps();   // replaces the reference steps in tau_ / sigma_

@@ -139,8 +139,8 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     m_ = lp.num_rows;
     n_ = lp.num_cols;
     PB_CUDA_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    PB_CUDA_CHECK(cudaMallocHost(&h_slots_, sizeof(double) * kSlotCount));
-    PB_CUDA_CHECK(cudaMallocHost(&h_status_, sizeof(int)));
+    PB_CUDA_CHECK(pinned_alloc(&h_slots_, sizeof(double) * kSlotCount));
+    PB_CUDA_CHECK(pinned_alloc(&h_status_, sizeof(int)));
     status_.alloc(1);
     slots_.alloc(kSlotCount);
     PB_CUDA_CHECK(cudaMemsetAsync(status_.get(), 0, sizeof(int), st_));
@@ -274,9 +274,12 @@ PdhgEngine::~PdhgEngine() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (graph_) cudaGraphDestroy(graph_);
     for (auto& e : ev_pool_) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
-    if (h_slots_) cudaFreeHost(h_slots_);
-    if (h_status_) cudaFreeHost(h_status_);
-    if (h_red_) cudaFreeHost(h_red_);
+    {
+        DeviceSyncScope gate;
+        if (h_slots_) cudaFreeHost(h_slots_);
+        if (h_status_) cudaFreeHost(h_status_);
+        if (h_red_) cudaFreeHost(h_red_);
+    }
     if (st_) cudaStreamDestroy(st_);
 }
 
@@ -369,16 +372,19 @@ double PdhgEngine::bytes_primal() const {
 void PdhgEngine::build_graph(int k) {
     if (graph_exec_) { cudaGraphExecDestroy(graph_exec_); graph_exec_ = nullptr; }
     if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
-    PB_CUDA_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-    try {
-        for (int i = 0; i < k; ++i) iterate_once();
-    } catch (...) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(st_, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
+    {
+        CaptureScope capture;
+        PB_CUDA_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int i = 0; i < k; ++i) iterate_once();
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        PB_CUDA_CHECK(cudaStreamEndCapture(st_, &graph_));
     }
-    PB_CUDA_CHECK(cudaStreamEndCapture(st_, &graph_));
     PB_CUDA_CHECK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
     graph_iters_ = k;
 }

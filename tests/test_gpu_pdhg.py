@@ -151,3 +151,37 @@ def test_large_zipf_iteration_properties():
     rx, ry, _ = oracle.trajectory(model, 1)
     np.testing.assert_allclose(y, ry, rtol=1e-4, atol=1e-4 * (1 + np.abs(ry).max()))
     np.testing.assert_allclose(x, rx, rtol=1e-4, atol=1e-4)
+
+
+def test_concurrent_solves_from_threads_match_sequential_solves():
+    """The reference serialises its GPU solves on the legacy default stream;
+    the backend interface it exposes requires concurrent solves on one
+    instance to be safe (include/pramaan/gpu/backend.hpp:33-35).  Here every
+    solve owns a stream, and the library's shared state (device-memory cache,
+    remembered launch shapes, occupancy queries) is guarded.  Solves started
+    from four threads at once (ctypes releases the GIL during the call) give
+    bit-identical answers to the same solves run one after another, in the
+    reference algorithm and in the batched Halpern mode."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from pramaan_b200 import solve_batch
+    from pramaan_b200.generators import random_sparse_lp, rolling_horizon_batch
+    from pramaan_b200.pdhg import ALGO_HALPERN
+
+    ref_models = [random_sparse_lp(400, 1200, 4, seed=s) for s in range(4)]
+    o = PdhgOptions(tolerance=1e-5, max_iterations=30000)
+    seq = [PdhgSolver(o).solve(md) for md in ref_models]
+    with ThreadPoolExecutor(4) as ex:
+        par = list(ex.map(lambda md: PdhgSolver(o).solve(md), ref_models))
+    for a, b in zip(seq, par):
+        assert a.status == b.status and a.iterations == b.iterations
+        assert np.array_equal(a.x, b.x) and a.objective_value == b.objective_value
+
+    batches = [rolling_horizon_batch(3, seed=40 + s, T_range=(24, 40), P_range=(5, 8)) for s in range(4)]
+    oh = PdhgOptions(tolerance=1e-6, max_iterations=200000, check_frequency=64, algorithm=ALGO_HALPERN)
+    seq = [solve_batch(b, oh) for b in batches]
+    with ThreadPoolExecutor(4) as ex:
+        par = list(ex.map(lambda b: solve_batch(b, oh), batches))
+    for sa, pa in zip(seq, par):
+        for a, b in zip(sa, pa):
+            assert a.iterations == b.iterations and np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
