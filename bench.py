@@ -758,6 +758,8 @@ def _hints_for(batch, prev):
 def run_gpu_arm(args):
     import torch
 
+    t_start = time.perf_counter()
+
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     dist = None
@@ -910,24 +912,34 @@ def run_gpu_arm(args):
     # shard over the ranks); the single-LP sections are replicas and run on
     # one GPU only.
     single = world == 1
+    wall = {"headline_and_e2e": time.perf_counter() - t_start}
+
+    def section(key, fn, *a):
+        t0 = time.perf_counter()
+        line[key] = fn(*a)
+        wall[key] = time.perf_counter() - t0
+
     if single and not args.no_banded:
-        line["banded_spmv"] = banded_section(args, local)
+        section("banded_spmv", banded_section, args, local)
     if single and not args.no_rolling:
-        line["small_lp"] = small_lp_section(args, local)
+        section("small_lp", small_lp_section, args, local)
     if single and not args.no_ladder:
-        line["ladder_lp"] = ladder_section(args, local)
+        section("ladder_lp", ladder_section, args, local)
     if not args.no_rolling:
-        line["rolling_horizon"] = rolling_horizon_section(args, local, dist)
+        section("rolling_horizon", rolling_horizon_section, args, local, dist)
     if single and not args.no_rolling:
-        line["batched_products"] = batch_iteration_section(args, local)
+        section("batched_products", batch_iteration_section, args, local)
     if single and not args.no_rolling:
-        line["learned_stream"] = learned_stream_section(args, local)
-        line["gnn_throughput"] = gnn_section(args, local)
+        section("learned_stream", learned_stream_section, args, local)
+        section("gnn_throughput", gnn_section, args, local)
     if rank == 0 and single and not args.no_cpu_baseline:
+        t0 = time.perf_counter()
         v, threads, sample = cpu_baseline(model, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": sample,
                                 "reference_solvers": reference_solvers_section(args, local)}
+        wall["cpu_baseline"] = time.perf_counter() - t0
+    line["section_wall_s"] = {k: round(v, 1) for k, v in wall.items()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

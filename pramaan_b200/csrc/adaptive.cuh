@@ -145,10 +145,14 @@ struct EpiPrimalAdapt {
 // written per element on the iterations that ask for it (fpr != nullptr).
 constexpr float kHalpernReflection = 1.0f;
 
+// Halpern weight of LP q at iteration offset of the interval.
+__device__ __forceinline__ float halpern_weight_lp(const int* iter_base, int offset, const int* restart_iter, int q) {
+    const long long k = (long long)(*iter_base) + offset - restart_iter[q];
+    return k <= 0 ? 0.5f : float(double(k + 1) / double(k + 2));
+}
 __device__ __forceinline__ float halpern_weight(const int* iter_base, int offset, const int* restart_iter,
                                                 const int* lp, int i) {
-    const long long k = (long long)(*iter_base) + offset - restart_iter[lp ? lp[i] : 0];   // lp null: one LP
-    return k <= 0 ? 0.5f : float(double(k + 1) / double(k + 2));
+    return halpern_weight_lp(iter_base, offset, restart_iter, lp ? lp[i] : 0);   // lp null: one LP
 }
 
 struct EpiPrimalHalpern {
@@ -174,7 +178,9 @@ struct EpiPrimalHalpern {
     // (the tile loop loads several columns ahead of their updates).
     static constexpr bool kSplit = true;
     struct In { float x_prev, t, c, lo, hi, a, w; };
-    __device__ In load(int j) const {
+    // w: the Halpern weight of column j's LP (halpern_weight), when the
+    // caller has it already
+    __device__ In load(int j, float w) const {
         In in;
         in.x_prev = x[j];
         in.t = tau[j];
@@ -182,9 +188,10 @@ struct EpiPrimalHalpern {
         in.lo = l_x[j];
         in.hi = u_x[j];
         in.a = anchor ? anchor[j] : 0.0f;
-        in.w = halpern_weight(iter_base, offset, restart_iter, lp, j);
+        in.w = w;
         return in;
     }
+    __device__ In load(int j) const { return load(j, halpern_weight(iter_base, offset, restart_iter, lp, j)); }
     __device__ void store(State&, int j, const In& in, float aty) const {
         if (!(in.t > 0.0f)) {        // a frozen LP keeps its iterate
             x_bar[j] = in.x_prev;
@@ -225,7 +232,7 @@ struct EpiDualHalpern {
     }
     static constexpr bool kSplit = true;
     struct In { float s, e_prev, ym, hi, lo, a, w; };
-    __device__ In load(int i) const {
+    __device__ In load(int i, float w) const {
         In in;
         in.s = sigma[i];
         in.e_prev = e[i];
@@ -233,9 +240,10 @@ struct EpiDualHalpern {
         in.hi = r_hi[i];
         in.lo = r_lo[i];
         in.a = anchor ? anchor[i] : 0.0f;
-        in.w = halpern_weight(iter_base, offset, restart_iter, lp, i);
+        in.w = w;
         return in;
     }
+    __device__ In load(int i) const { return load(i, halpern_weight(iter_base, offset, restart_iter, lp, i)); }
     __device__ void store(State&, int i, const In& in, float ad) const {
         const float s = in.s;
         const float e_prev = in.e_prev;

@@ -877,6 +877,42 @@ void AdaptiveBatch::build_cluster_lps() {
     }
     cluster_size_ = C;
     cluster_auto_ = cluster_auto_ && C >= kClusterAutoMin;
+    if (use_cluster_kernel()) build_cluster_long_rows(v);
+}
+
+void AdaptiveBatch::build_cluster_long_rows(const std::vector<int4>& lps) {
+    std::vector<int> rp(size_t(m_) + 1, 0), cp(size_t(n_) + 1, 0);
+    if (m_ > 0)
+        PB_CUDA_CHECK(cudaMemcpyAsync(rp.data(), A_.row_ptr.get(), rp.size() * sizeof(int), cudaMemcpyDeviceToHost, st_));
+    if (n_ > 0)
+        PB_CUDA_CHECK(cudaMemcpyAsync(cp.data(), AT_.row_ptr.get(), cp.size() * sizeof(int), cudaMemcpyDeviceToHost, st_));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st_));
+    std::vector<int4> range;
+    std::vector<int> la, lat;
+    for (const int4& q : lps) {
+        int4 r;
+        r.x = int(la.size());
+        for (int i = q.x; i < q.y; ++i)
+            if (rp[size_t(i) + 1] - rp[size_t(i)] > kClusterLongRow) la.push_back(i);
+        r.y = int(la.size());
+        r.z = int(lat.size());
+        for (int j = q.z; j < q.w; ++j)
+            if (cp[size_t(j) + 1] - cp[size_t(j)] > kClusterLongRow) lat.push_back(j);
+        r.w = int(lat.size());
+        range.push_back(r);
+    }
+    cluster_long_range_.alloc(range.empty() ? 1 : range.size());
+    cluster_long_a_.alloc(la.empty() ? 1 : la.size());
+    cluster_long_at_.alloc(lat.empty() ? 1 : lat.size());
+    if (!range.empty())
+        PB_CUDA_CHECK(cudaMemcpyAsync(cluster_long_range_.get(), range.data(), range.size() * sizeof(int4),
+                                      cudaMemcpyHostToDevice, st_));
+    if (!la.empty())
+        PB_CUDA_CHECK(cudaMemcpyAsync(cluster_long_a_.get(), la.data(), la.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
+    if (!lat.empty())
+        PB_CUDA_CHECK(cudaMemcpyAsync(cluster_long_at_.get(), lat.data(), lat.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, st_));
+    PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // the host lists are freed on return
 }
 
 bool AdaptiveBatch::use_cluster_kernel() const {
@@ -909,7 +945,12 @@ void AdaptiveBatch::launch_cluster(int k) {
     const int4* lps = cluster_lps_.get();
     const float* yp = y_.get();
     const float* xb = xbar_.get();
-    PB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, halpern_cluster_kernel, lps, fa, fat, ep, ed, yp, xb, k, c0, c1, r0, r1));
+    const int4* lr = cluster_long_range_.get();
+    const int* la = cluster_long_a_.get();
+    const int* lat = cluster_long_at_.get();
+    if (!lr || !la || !lat) throw std::logic_error("cluster kernel: long-row lists missing");
+    PB_CUDA_CHECK(cudaLaunchKernelEx(&cfg, halpern_cluster_kernel, lps, lr, la, lat, fa, fat, ep, ed, yp, xb, k, c0,
+                                     c1, r0, r1));
 }
 
 void AdaptiveBatch::iterate(int k, int iter) {

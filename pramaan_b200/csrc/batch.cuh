@@ -102,6 +102,8 @@ private:
     // current layout and picks the cluster size.
     bool use_cluster_kernel() const;
     void build_cluster_lps();
+    // the long-row lists of the cluster kernel for the LPs `lps` ({r0, r1, c0, c1})
+    void build_cluster_long_rows(const std::vector<int4>& lps);
     void launch_cluster(int k);
     void solve_halpern();
     void materialize_average();
@@ -157,6 +159,10 @@ private:
     bool cluster_auto_ = false;              // every LP small enough for the automatic choice
     int cluster_nlps_ = 0, cluster_size_ = 1;
     DevBuf<int4> cluster_lps_;               // {r0, r1, c0, c1} per LP of the current layout
+    // rows of A and of A^T longer than kClusterLongRow, per LP of the current
+    // layout (ranges {a0, a1, at0, at1} into the two lists)
+    DevBuf<int4> cluster_long_range_;
+    DevBuf<int> cluster_long_a_, cluster_long_at_;
     DevBuf<double> xw_, yw_;           // warm start (original layout), empty when cold
     DevBuf<double> inv_;
     DevBuf<float> dscale_, pscale_, lp_f_;
