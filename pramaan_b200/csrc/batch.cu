@@ -824,11 +824,12 @@ void AdaptiveBatch::launch_interval(int k) {
 // tail of a batch, or a single LP) and every LP has at most
 // kClusterAutoMaxNnz non-zeros; persistent = 2 takes it always.  Measured on
 // the rolling-horizon batch (128 LPs, T ~ U{24..336}, P ~ U{5..50}): its
-// slowest LP alone (66,704 non-zeros, 300 k iterations) at 16.9 us per
-// iteration against 19.5 on the tiled path, its 2 and 5 slowest LPs at 17.9 /
-// 20.5 against 22.2 / 24.9 us; with one block per LP (the whole batch) the
-// cluster kernel was 4x slower than the packed tiled products, whose grid
-// spreads every LP over the whole GPU.
+// slowest LP alone (66,704 non-zeros, 300 k iterations) at 10.1 us per
+// iteration against 17.9 on the tiled path; its first 16 and 32 LPs (clusters
+// of 8 and 4 blocks) at 18.1 / 30.3 against 24.0 / 46.5 us, but 64 and 128
+// LPs (2 blocks, 1 block) at 68.7 / 141.5 against 44.5 / 72.9 us, where the
+// packed tiled products spread every LP over the whole GPU.  Clusters of 4 or
+// 2 blocks taking the tail earlier did not change the 512-LP batch's time.
 constexpr long long kClusterAutoMaxNnz = 1LL << 20;
 // Halpern mode compacts the operand once the LPs still iterating hold less
 // than this share of its non-zeros (a compaction costs ~0.1 s on the 512-LP

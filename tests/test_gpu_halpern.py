@@ -147,6 +147,49 @@ def test_cluster_kernel_follows_the_tiled_path():
         assert ra.iterations == rc.iterations and np.array_equal(ra.x, rc.x) and np.array_equal(ra.y, rc.y)
 
 
+def _long_rows_and_columns_lp(seed=0):
+    """400 x 1200 LP with three entries per column plus one row of 300
+    entries, five rows of 40 and ten columns of 100 (rows and columns longer
+    than the cluster kernel's one-thread limit of 16 entries, one past two
+    64-entry warp steps), feasible and bounded by construction."""
+    from pramaan_b200.generators import _csr_from_coo, _distinct_rows_per_col, _feasible_model
+
+    rng = np.random.default_rng(seed)
+    m, n = 400, 1200
+    pairs = {(int(r), j) for j in range(n) for r in _distinct_rows_per_col(rng, m, 1, 3)[0]}
+    pairs |= {(0, int(j)) for j in rng.choice(n, 300, replace=False)}
+    for r in range(1, 6):
+        pairs |= {(r, int(j)) for j in rng.choice(n, 40, replace=False)}
+    for j in range(10):
+        pairs |= {(int(r), j) for r in rng.choice(m, 100, replace=False)}
+    rows = np.array([p[0] for p in pairs])
+    cols = np.array([p[1] for p in pairs])
+    vals = rng.standard_normal(rows.size)
+    rp, ci, va = _csr_from_coo(rows, cols, vals, m)
+    return _feasible_model(rng, m, n, rp, ci, va)[0]
+
+
+def test_cluster_kernel_long_rows_and_columns():
+    """Rows and columns past 16 entries go one warp each (lists built on the
+    host); every row and column is still updated once per iteration, so the
+    iterates follow the tiled path to FP32 rounding and the solve certifies."""
+    md = _long_rows_and_columns_lp()
+    lens = np.diff(np.asarray(md.row_ptr))
+    assert lens.max() >= 300 and (np.bincount(np.asarray(md.col_idx)) > 16).sum() >= 10
+    models = [md, random_sparse_lp(300, 900, 4, seed=2)]
+    short = dict(tolerance=0.0, max_iterations=64, check_frequency=64, algorithm=ALGO_HALPERN)
+    a = solve_batch(models, PdhgOptions(persistent=2, **short))
+    b = solve_batch(models, PdhgOptions(persistent=-1, **short))
+    for ra, rb in zip(a, b):
+        assert np.allclose(ra.x, rb.x, rtol=1e-4, atol=1e-4 * (1 + np.abs(rb.x).max()))
+        assert np.allclose(ra.y, rb.y, rtol=1e-4, atol=1e-4 * (1 + np.abs(rb.y).max()))
+    full = dict(tolerance=1e-7, max_iterations=400000, check_frequency=64, algorithm=ALGO_HALPERN)
+    r = solve_batch([md], PdhgOptions(persistent=2, **full))[0]
+    assert r.status == SolveStatus.kOptimal
+    k = oracle.rel_kkt(md, r.x, r.y)
+    assert max(k["primal"], k["dual"], k["gap"]) <= 1e-7 * 1.0001
+
+
 def test_cluster_kernel_single_lp_and_one_lp_left():
     """A single LP (a batch of one gets the largest cluster) and a batch whose
     compaction leaves one slow LP alone: answers certified and equal to the
