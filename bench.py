@@ -85,7 +85,8 @@ def parse():
     p.add_argument("--launch-blocks", type=int, default=0,
                    help="fixed blocks per SM of the products (0: autotuned); with --gather-cache 1 or -1 "
                         "the launch shape is fixed, for profiles")
-    p.add_argument("--only", default=None, choices=["banded", "gnn", "small", "rolling", "stream", "ceiling", "ladder", "solvers", "batch"],
+    p.add_argument("--only", default=None, choices=["banded", "gnn", "small", "rolling", "stream", "ceiling", "ladder", "solvers", "batch",
+                            "tail"],
                    help="run one section alone on the given sizes and print its JSON (profiling runs)")
     p.add_argument("--gnn-lps", type=int, default=64, help="rolling-horizon LPs of the network throughput section")
     p.add_argument("--gnn-reps", type=int, default=5)
@@ -443,6 +444,45 @@ def batch_iteration_section(args, device, models=None):
             "peak_gbs": hbm, "peak_kind": kind}
 
 
+def batch_tail_section(args, device):
+    """The batch's tail: the 128-LP rolling-horizon batch's largest LP, and
+    its two largest together, iterated by the per-LP cluster kernel (the
+    default once a batch is down to a few LPs) and by the packed tiled
+    products, each for a fixed number of iterations (tolerance 0) and timed
+    as the difference of a 4K- and a K-iteration solve, checks every 64
+    iterations included."""
+    import torch
+
+    from pramaan_b200 import PdhgOptions, solve_batch
+    from pramaan_b200.generators import rolling_horizon_batch
+    from pramaan_b200.pdhg import ALGO_HALPERN
+
+    batch = rolling_horizon_batch(128, seed=args.seed)
+    order = sorted(range(len(batch)), key=lambda i: -batch[i].nnz())
+    K = 640
+    out = {"workload": f"rolling_horizon_batch 128 LPs (seed {args.seed}): its largest LP and its two largest, "
+                       f"{K} vs {4 * K} iterations, median of 3"}
+    for tag, idx in (("largest", order[:1]), ("two_largest", order[:2])):
+        models = [batch[i] for i in idx]
+        row = {"rows": sum(m.numRows() for m in models), "cols": sum(m.numVars() for m in models),
+               "nnz": sum(m.nnz() for m in models)}
+        for path, persistent in (("cluster_kernel", 2), ("tiled", -1)):
+            def run(k):
+                o = PdhgOptions(tolerance=0.0, max_iterations=k, check_frequency=64, algorithm=ALGO_HALPERN,
+                                device=device, persistent=persistent)
+                t0 = time.perf_counter()
+                solve_batch(models, o)
+                return time.perf_counter() - t0
+            run(K)   # warm-up
+            torch.cuda.nvtx.range_push("timed")
+            a = sorted(run(K) for _ in range(3))[1]
+            b = sorted(run(4 * K) for _ in range(3))[1]
+            torch.cuda.nvtx.range_pop()
+            row[f"{path}_us_per_iteration"] = (b - a) / (3 * K) * 1e6
+        out[tag] = row
+    return out
+
+
 def learned_stream_section(args, device):
     """S streams of rolling-horizon windows solved step by step (window w of
     every stream is one batch), cold against the certified learned warm start
@@ -778,7 +818,7 @@ def run_gpu_arm(args):
                     "stream": learned_stream_section,
                     "ceiling": lambda a, d: gather_ceiling(a.n, d),
                     "ladder": ladder_section, "solvers": reference_solvers_section,
-                    "batch": batch_iteration_section,
+                    "batch": batch_iteration_section, "tail": batch_tail_section,
                     "rolling": lambda a, d: rolling_horizon_section(a, d, dist)}
         out = sections[args.only](args, local)
         if rank == 0:
@@ -929,6 +969,7 @@ def run_gpu_arm(args):
         section("rolling_horizon", rolling_horizon_section, args, local, dist)
     if single and not args.no_rolling:
         section("batched_products", batch_iteration_section, args, local)
+        section("batch_tail", batch_tail_section, args, local)
     if single and not args.no_rolling:
         section("learned_stream", learned_stream_section, args, local)
         section("gnn_throughput", gnn_section, args, local)
