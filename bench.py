@@ -77,8 +77,13 @@ def parse():
     p.add_argument("--stream-T", type=int, nargs=2, default=(24, 336), help="periods of the stream windows")
     p.add_argument("--stream-P", type=int, nargs=2, default=(5, 50), help="products of the stream windows")
     p.add_argument("--weights", default=None, help="warm-start network weights (.npz; default: the committed ones)")
+    p.add_argument("--learned-tail", type=int, default=4,
+                   help="periods at the end of each window where the network's prediction replaces the shifted "
+                        "previous solution (0: the network everywhere, the certificate choosing between "
+                        "candidate starts after --probe-iters iterations)")
     p.add_argument("--probe-iters", type=int, default=64,
-                   help="PDHG iterations from each candidate start before the certificate chooses")
+                   help="with --learned-tail 0: PDHG iterations from each candidate start before the certificate "
+                        "chooses")
     p.add_argument("--no-rolling", action="store_true", help="skip both rolling-horizon sections")
     p.add_argument("--no-banded", action="store_true", help="skip the banded-LP bandwidth section")
     p.add_argument("--banded-iters", type=int, default=50)
@@ -511,7 +516,10 @@ def learned_stream_section(args, device):
                        f"10,000-window stream), rel KKT {tol:g}; window w of every stream is one batch",
            "trained_on": {k: rec[k] for k in ("instances_solved", "instances_trained", "epochs", "T", "P")
                           if k in rec},
-           "probe_iterations": args.probe_iters}
+           "learned_start": (f"the network's prediction on the last {args.learned_tail} periods of each window, "
+                             "the shifted previous solution elsewhere" if args.learned_tail > 0 else
+                             f"the certificate's choice among the network's point, the hint, their midpoint and "
+                             f"cold after {args.probe_iters} probe iterations each")}
     solve_batch(windows[0][:2], o)                   # warm-up
     # the plain per-LP solver on a sample of the same windows
     from pramaan_b200 import PdhgSolver
@@ -535,7 +543,11 @@ def learned_stream_section(args, device):
             elif mode == "hint":
                 res = solve_batch(batch, o, warm=hints)
             else:
-                res, info = warm_solve_batch(batch, net, o, hints=hints, probe_iterations=args.probe_iters)
+                if args.learned_tail > 0:
+                    res, info = warm_solve_batch(batch, net, o, hints=hints, select=False,
+                                                 refine_masks=_tail_masks(batch, hints, args.learned_tail))
+                else:
+                    res, info = warm_solve_batch(batch, net, o, hints=hints, probe_iterations=args.probe_iters)
                 for c in info.choices:
                     choices[c] = choices.get(c, 0) + 1
                 for k in phases:
@@ -774,6 +786,18 @@ def gnn_section(args, device):
             "dense_forward_flops": fwd_flops, "dense_train_flops": 3 * fwd_flops,
             "dense_forward_bytes": layers * 384 * (m + n),
             "nodes_per_s_forward": (m + n) / t_fwd, "nodes_per_s_train": (m + n) / t_step}
+
+
+def _tail_masks(batch, hints, k):
+    """The last k periods of every window that has a hint (rolling_horizon_lp layout)."""
+    from pramaan_b200.generators import rolling_horizon_tail_mask
+
+    out = []
+    for md, h in zip(batch, hints):
+        PT = md.numVars() // 3
+        T = md.numRows() - PT
+        out.append(None if h is None else rolling_horizon_tail_mask(T, PT // T, k))
+    return out
 
 
 def _hints_for(batch, prev):

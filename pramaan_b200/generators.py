@@ -323,3 +323,14 @@ def rolling_horizon_shift(x, y, T: int, P: int):
     y = np.asarray(y, np.float64)
     ys = np.concatenate([sh(y[:P * T], (P,)), sh(y[P * T:], (1,))])
     return xs, ys
+
+
+def rolling_horizon_tail_mask(T: int, P: int, k: int):
+    """(x_mask, y_mask) of the last k periods of a window in the layout of
+    ``rolling_horizon_lp``: the periods a shifted previous solution knows
+    least about (the new last period is only a copy, and the ones before it
+    carried the previous window's end-of-horizon effects)."""
+    k = max(0, min(int(k), T))
+    tail = np.zeros(T, bool)
+    tail[T - k:] = True
+    return np.tile(tail, 3 * P), np.concatenate([np.tile(tail, P), tail])

@@ -257,22 +257,41 @@ def select_starts(models: list[ModelIR], candidates: dict[str, list], device: in
     return starts, chosen, kkt, spent
 
 
+def splice_refinement(hint: WarmStart | None, pred: WarmStart | None, mask) -> WarmStart | None:
+    """The hint with the network's values where ``mask`` = (x_mask, y_mask) is
+    set (None: the network's point everywhere)."""
+    if hint is None or pred is None or mask is None:
+        return pred
+    xm, ym = mask
+    x = np.where(xm, pred.x, np.asarray(hint.x, np.float64))
+    y = None if hint.y is None else np.where(ym, pred.y, np.asarray(hint.y, np.float64))
+    return WarmStart(x, y, 0.0)
+
+
 def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOptions,
                      fallback_iterations: int | None = None,
                      hints: list[WarmStart | None] | None = None,
                      use_predicted_weight: bool = False,
-                     probe_iterations: int = 0) -> tuple[list[SolveResult], WarmSolveInfo]:
+                     probe_iterations: int = 0,
+                     refine_masks: list | None = None,
+                     select: bool = True) -> tuple[list[SolveResult], WarmSolveInfo]:
     """Learned warm start, certified, with the cold start as fallback.
 
     1. The network predicts (x, y, omega) for every LP (refining ``hints``
-       when given, see ``GnnGraph``).
-    2. The certificate decides the start of each LP: the network's point, the
-       hint, (when probing) the point halfway between them, or the cold start,
-       whichever has the smallest FP64 relative KKT error (``select_starts``),
-       judged after ``probe_iterations`` PDHG
+       when given, see ``GnnGraph``).  With ``refine_masks`` (one
+       (x_mask, y_mask) or None per LP) its point is taken only where the
+       mask is set and the hint elsewhere (``splice_refinement``): on
+       rolling-horizon windows the network then predicts the tail of the
+       horizon, which the previous window's solution cannot supply, and
+       leaves the periods that solution already has to it.
+    2. With ``select`` the certificate decides the start of each LP: the
+       network's point, the hint, (when probing) the point halfway between
+       them, or the cold start, whichever has the smallest FP64 relative KKT
+       error (``select_starts``), judged after ``probe_iterations`` PDHG
        iterations from each when that is > 0 (the solve then continues from
        the chosen probe's point; every probe's iterations are counted in
-       ``WarmSolveInfo.probe_iterations``).
+       ``WarmSolveInfo.probe_iterations``).  Without ``select`` every LP
+       starts from the network's point (the cold start where there is none).
     3. The batch is solved from those starts (with the predicted primal
        weight when ``use_predicted_weight``, else the solver's default).
     4. Every LP whose solve is not optimal (it hit ``options.max_iterations``)
@@ -283,8 +302,17 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
 
     t0 = time.perf_counter()
     pred = net.predict(models, hints=hints)
+    if refine_masks is not None:
+        if hints is None or len(refine_masks) != len(models):
+            raise ValueError("warm_solve_batch: refine_masks needs hints and one mask (or None) per LP")
+        pred = [splice_refinement(h, p, mk) for h, p, mk in zip(hints, pred, refine_masks)]
     t1 = time.perf_counter()
     cands = {"network": pred}
+    if not select:
+        res, info = _solve_from(models, options, pred, ["network" if p is not None else "cold" for p in pred],
+                                [float("nan")] * len(models), pred, use_predicted_weight, fallback_iterations,
+                                t0, t1, time.perf_counter(), 0)
+        return res, info
     if hints is not None:
         cands["hint"] = list(hints)
         # halfway between the hint and the network's refinement of it: the
@@ -294,14 +322,23 @@ def warm_solve_batch(models: list[ModelIR], net: WarmStartNet, options: PdhgOpti
                               WarmStart(0.5 * (np.asarray(h.x) + p.x), 0.5 * (np.asarray(h.y) + p.y), 0.0)
                               for h, p in zip(hints, pred)]
     starts, chosen, kkt, spent = select_starts(models, cands, net.device, probe_iterations, options)
+    return _solve_from(models, options, starts, chosen, kkt, pred, use_predicted_weight, fallback_iterations,
+                       t0, t1, time.perf_counter(), spent)
+
+
+def _solve_from(models, options, starts, chosen, kkt, pred, use_predicted_weight, fallback_iterations,
+                t0, t1, t_sel, spent):
+    """Steps 3 and 4 of ``warm_solve_batch``."""
+    import time
+
     warm = []
-    for st, nm, p in zip(starts, chosen, pred):
+    for st, p in zip(starts, pred):
         if st is None:
             warm.append(None)
         else:
             w = p.primal_weight if (use_predicted_weight and p is not None) else 0.0
             warm.append(WarmStart(st.x, st.y, w))
-    t2 = time.perf_counter()
+    t2 = t_sel
     res = solve_batch(models, options, warm=warm)
     t3 = time.perf_counter()
     warm_its = [r.iterations for r in res]

@@ -4,7 +4,8 @@ import numpy as np
 import pytest
 
 import oracle
-from pramaan_b200.generators import random_sparse_lp, rolling_horizon_batch, rolling_horizon_lp
+from pramaan_b200.generators import (random_sparse_lp, rolling_horizon_batch, rolling_horizon_lp,
+                                    rolling_horizon_shift, rolling_horizon_tail_mask)
 
 
 def test_rolling_horizon_structure():
@@ -59,3 +60,34 @@ def test_rolling_horizon_small_solved_by_reference_simplex():
 def test_random_sparse_lp_feasible_by_construction():
     m, cert = random_sparse_lp(50, 150, 4, seed=2, return_certificate=True)
     np.testing.assert_allclose(m.multiply(cert["x0"]), m.row_lower, rtol=1e-12, atol=1e-9)
+
+
+def test_rolling_horizon_tail_mask_and_splice():
+    """The tail mask selects the last k periods of every block of the
+    rolling-horizon layout (three variable blocks of P x T, P balance rows of
+    T, then T capacity rows); the spliced start takes the network's values
+    there and the hint's elsewhere.  The period the shift only copies is
+    always inside a non-empty tail."""
+    from pramaan_b200.gnn import WarmStart, splice_refinement
+
+    T, P = 7, 3
+    md = rolling_horizon_lp(T, P, seed=1)
+    assert md.numVars() == 3 * P * T and md.numRows() == P * T + T
+    xm, ym = rolling_horizon_tail_mask(T, P, 2)
+    assert xm.shape == (3 * P * T,) and ym.shape == (P * T + T,)
+    t = np.tile(np.arange(T), 3 * P)
+    assert np.array_equal(xm, t >= T - 2)
+    assert np.array_equal(ym, np.concatenate([np.tile(np.arange(T), P), np.arange(T)]) >= T - 2)
+    assert not rolling_horizon_tail_mask(T, P, 0)[0].any() and rolling_horizon_tail_mask(T, P, 99)[1].all()
+    rng = np.random.default_rng(0)
+    x, y = rng.standard_normal(3 * P * T), rng.standard_normal(P * T + T)
+    xs, ys = rolling_horizon_shift(x, y, T, P)
+    copied = np.tile(np.arange(T), 3 * P) == T - 1
+    assert np.array_equal(xs[copied], x[np.tile(np.arange(T), 3 * P) == T - 1])
+    assert xm[copied].all()
+    hint = WarmStart(xs, ys, 0.0)
+    pred = WarmStart(rng.standard_normal(xs.size), rng.standard_normal(ys.size), 2.0)
+    sp = splice_refinement(hint, pred, (xm, ym))
+    assert np.array_equal(sp.x, np.where(xm, pred.x, xs)) and np.array_equal(sp.y, np.where(ym, pred.y, ys))
+    assert sp.primal_weight == 0.0
+    assert splice_refinement(hint, pred, None) is pred and splice_refinement(None, pred, (xm, ym)) is pred

@@ -14,7 +14,8 @@ import pytest
 from lp_cases import KNOWN
 from oracle import gnn as og
 from pramaan_b200 import PdhgOptions, SolveStatus, solve_batch
-from pramaan_b200.generators import random_sparse_lp, rolling_horizon_batch, rolling_horizon_lp
+from pramaan_b200.generators import (random_sparse_lp, rolling_horizon_batch, rolling_horizon_lp,
+                                    rolling_horizon_tail_mask)
 from pramaan_b200.gnn import WarmStart, WarmStartNet, training_targets, warm_solve_batch
 from pramaan_b200.pdhg import ALGO_ADAPTIVE
 
@@ -252,9 +253,11 @@ def test_learned_start_measured_against_the_hint_it_refines():
     start.  On held-out streams both are measured in total PDHG iterations,
     the learned pipeline's probes included.  The network's refinement is not
     a reliable gain over the hint it refines (on the benchmark stream it
-    needs 5 % more iterations), so what is asserted is that the
-    certified pipeline never falls far behind the hint, that both beat cold
-    starts, and that every answer is certified."""
+    needs 5 % more iterations), and neither is the network confined to the
+    last periods of each window (the hint elsewhere): within a few per cent
+    of the hint either way on held-out streams.  So what is asserted is that
+    both learned pipelines stay close to the hint, that all beat cold starts,
+    and that every answer is certified."""
     from pramaan_b200.certificate import certify_batch
     from pramaan_b200.train_warm_start import DEFAULT_OUT
     o = opts()
@@ -269,11 +272,20 @@ def test_learned_start_measured_against_the_hint_it_refines():
     cold_total = sum(r.iterations for r in cold)
     hint_total = sum(r.iterations for r in hint)
     learned_total = sum(info.warm_iterations) + info.probe_iterations
+    # the network on the last four periods of each window only, the hint elsewhere, no selection
+    masks = []
+    for md, h in zip(ev, hev):
+        T = md.numRows() - md.numVars() // 3
+        masks.append(None if h is None else rolling_horizon_tail_mask(T, md.numVars() // (3 * T), 4))
+    res_t, info_t = warm_solve_batch(ev, net, o, hints=hev, refine_masks=masks, select=False)
+    tail_total = sum(info_t.warm_iterations)
     print(f"iterations: cold {cold_total}, hint {hint_total} ({hint_total / cold_total:.3f}), learned "
           f"{learned_total} ({learned_total / cold_total:.3f}, {learned_total / hint_total:.3f} of hint); "
-          f"starts {dict((c, info.choices.count(c)) for c in set(info.choices))}")
-    assert hint_total < cold_total and learned_total < cold_total
-    assert learned_total <= 1.15 * hint_total
-    cert = certify_batch(ev, [[WarmStart(r.x, r.y) for r in res]])[0]
-    for r, c in zip(res, cert):
-        assert r.status == SolveStatus.kOptimal and c.kkt <= 1e-6 * 1.0001
+          f"starts {dict((c, info.choices.count(c)) for c in set(info.choices))}; network on the last 4 periods "
+          f"{tail_total} ({tail_total / hint_total:.3f} of hint)")
+    assert hint_total < cold_total and learned_total < cold_total and tail_total < cold_total
+    assert learned_total <= 1.15 * hint_total and tail_total <= 1.15 * hint_total
+    cert = certify_batch(ev, [[WarmStart(r.x, r.y) for r in res], [WarmStart(r.x, r.y) for r in res_t]])
+    for rr, cc in ((res, cert[0]), (res_t, cert[1])):
+        for r, c in zip(rr, cc):
+            assert r.status == SolveStatus.kOptimal and c.kkt <= 1e-6 * 1.0001
