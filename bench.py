@@ -95,6 +95,9 @@ def parse():
                    help="run one section alone on the given sizes and print its JSON (profiling runs)")
     p.add_argument("--gnn-lps", type=int, default=64, help="rolling-horizon LPs of the network throughput section")
     p.add_argument("--gnn-reps", type=int, default=5)
+    p.add_argument("--panel-split", type=int, default=0,
+                   help="A x̄ product: 0 column panels for the long rows of a power-law A (automatic), "
+                        "1 whenever feasible, >= 2 rows of that many entries as long rows, -1 tiled only")
     p.add_argument("--gather-cache", type=int, default=0, choices=[0, 1, -1],
                    help="0: hot gather targets in shared memory, L1-cached gathers where faster (the "
                         "default); 1: L1-cached gathers wherever there are no hot slots; -1: plain")
@@ -861,9 +864,10 @@ def run_gpu_arm(args):
     nnz = model.nnz()
 
     opts = PdhgOptions(device=local, use_graph=False, profile_kernels=True, gather_cache=args.gather_cache,
-                       launch_blocks=args.launch_blocks)
+                       launch_blocks=args.launch_blocks, panel_split=args.panel_split)
     sess = Session(model, opts)
     gather = sess.gather_info()
+    panel = sess.panel_info()
     stream = torch.cuda.ExternalStream(sess.stream(), device=local)
     for _ in range(args.warmup):
         sess.iterate(1)
@@ -912,11 +916,16 @@ def run_gpu_arm(args):
                 "frac": achieved / hbm, "peak_kind": peak_kind,
                 "traffic": ncu_traffic(f"{tag}_zipf_lp_2Mx5M"),
                 "algorithmic_bytes_per_launch": kbytes, "avg_launch_ms": avg_s * 1000,
-                "timed_span": "one product: its main kernel and its crossing-row completion kernel"}
+                "timed_span": ("one product: its main kernel and its crossing-row completion kernel"
+                               if not (tag == "spmv_dual_fused" and panel["panels"]) else
+                               "one A x̄ product: the column-panel kernel of the long rows, the short rows' "
+                               "tiled product and its completion kernel, the long rows' finish kernel")}
     other = [k for k in kinds if k[0] != tag][0]
     roofline["other_kernel"] = {"kernel": other[0], "achieved": other[2] / (other[1] / 1000 / args.steps) / 1e9,
                                 "frac": other[2] / (other[1] / 1000 / args.steps) / 1e9 / hbm,
                                 "avg_launch_ms": other[1] / args.steps}
+    if panel["panels"]:
+        roofline["dual_panel_split"] = {**panel, "long_share": panel["long_nnz"] / nnz}
     # Second roofline: every non-zero is one random 4-byte gather of x̄ (A x̄)
     # or y (Aᵀ y, whose hot targets are read from shared memory instead).
     ceil = gather_ceiling(args.n, local)
@@ -930,7 +939,7 @@ def run_gpu_arm(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**workload_config(args, nnz),
-                       "gather": gather},
+                       "gather": gather, "panel_split": panel},
             "gpu_launches": int(launches),
             "clocks": clk.summary(), "roofline": roofline,
             "residual_checks": {
@@ -953,7 +962,8 @@ def run_gpu_arm(args):
                      model.obj_sense, model.obj_offset)
         solver = pramaan_b200.PdhgSolver(PdhgOptions(device=local, tolerance=0.0,
                                                      max_iterations=args.e2e_iters, check_frequency=100,
-                                                     gather_cache=args.gather_cache))
+                                                     gather_cache=args.gather_cache,
+                                                     panel_split=args.panel_split))
         solver.solve(pm)   # warm-up (module load, first-touch)
         times = []
         for _ in range(args.e2e_calls):

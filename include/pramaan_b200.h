@@ -128,7 +128,20 @@ typedef struct pramaan_pdhg_options {
                                  and not even that when gather_cache is 1 or
                                  -1: a fixed launch shape, for reproducible
                                  profiles                                       */
-    int32_t reserved[3];
+    int32_t panel_split;      /* reference algorithm, the A x̄ product:
+                                 0 (default): when rows of at least half the
+                                 panel count of entries hold half or more of
+                                 A's non-zeros (power-law row lengths, at
+                                 least 4 Mi of them), those long rows are
+                                 computed over column panels of x̄ held in
+                                 shared memory, one per SM, and the other rows
+                                 by the tiled product; 1: the same split
+                                 whenever it is feasible; >= 2: the split with
+                                 rows of at least that many entries as the long
+                                 rows; -1: the tiled product only.  Sums are
+                                 deterministic in every mode; a split changes
+                                 the order of the additions within a row      */
+    int32_t reserved[2];
 } pramaan_pdhg_options;
 
 /* Result, mirroring pramaan::SolveResult (include/pramaan/simplex.hpp:40-76).
@@ -447,6 +460,14 @@ PRAMAAN_API int pramaan_measure_gather_rate(const float* d_x, int32_t n, int32_t
 PRAMAAN_API int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual,
                                 int32_t* slots_primal, int32_t* l1_dual, int32_t* l1_primal,
                                 int32_t* blocks_dual, int32_t* blocks_primal);
+
+/* Column-panel split of the dual product (option panel_split): the panels
+ * (one per SM; 0 when A x̄ runs as the tiled product alone), the long rows
+ * they compute, those rows' non-zeros, and the row length from which a row is
+ * long.  No reference counterpart (the reference computes A x̄ one thread per
+ * row).  Any pointer may be NULL. */
+PRAMAAN_API int pramaan_session_panel_info(pramaan_pdhg_session* s, int32_t* panels, int32_t* long_rows,
+                                           int64_t* long_nnz, int32_t* min_len);
 
 #ifdef __cplusplus
 }

@@ -36,7 +36,7 @@ class COptions(C.Structure):
         ("tolerance", f64), ("max_iterations", i32), ("check_frequency", i32),
         ("algorithm", i32), ("termination", i32), ("device", i32), ("use_graph", i32),
         ("profile_kernels", i32), ("refine", i32), ("reserved_d", f64),
-        ("persistent", i32), ("gather_cache", i32), ("launch_blocks", i32), ("reserved", i32 * 3),
+        ("persistent", i32), ("gather_cache", i32), ("launch_blocks", i32), ("panel_split", i32), ("reserved", i32 * 2),
     ]
 
 
@@ -119,6 +119,8 @@ SIGNATURES = [
      [P, C.POINTER(f64), C.POINTER(f64), C.POINTER(i64), i32]),
     ("pramaan_session_kernel_bytes", C.c_int, [P, C.POINTER(f64), C.POINTER(f64)]),
     ("pramaan_session_gather_info", C.c_int, [P] + [C.POINTER(i32)] * 6),
+    ("pramaan_session_panel_info", C.c_int, [P, C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_int64),
+                                             C.POINTER(i32)]),
     ("pramaan_release_cached_memory", C.c_int, [i32]),
     ("pramaan_measure_gather_rate", C.c_int, [P, i32, i32, i32, C.POINTER(f64)]),
 ]

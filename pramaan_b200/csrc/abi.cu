@@ -406,6 +406,20 @@ int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual, in
     });
 }
 
+int pramaan_session_panel_info(pramaan_pdhg_session* s, int32_t* panels, int32_t* long_rows, int64_t* long_nnz,
+                               int32_t* min_len) {
+    return guarded([&] {
+        if (!s) throw InvalidArgument("session is NULL");
+        int p = 0, l = 0, ml = 0;
+        long long nz = 0;
+        s->eng->panel_info(&p, &l, &nz, &ml);
+        if (panels) *panels = p;
+        if (long_rows) *long_rows = l;
+        if (long_nnz) *long_nnz = nz;
+        if (min_len) *min_len = ml;
+    });
+}
+
 int pramaan_measure_gather_rate(const float* d_x, int32_t n, int32_t cached, int32_t reps,
                                 double* gathers_per_s) {
     return guarded([&] {

@@ -140,6 +140,33 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
+// try_wait with a suspend-time hint: a thread whose phase has not completed
+// sleeps in hardware for up to `hint_ns` instead of returning at once, so
+// waiting warps do not take issue slots from the warps that have work.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait that sleeps between checks (see mbar_try_wait_sleep); gives
+// up after kWaitLimitNs like mbar_wait_bounded.
+__device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t* bar, uint32_t parity) {
+    constexpr uint32_t kHintNs = 20000;
+    if (mbar_try_wait_sleep(bar, parity, kHintNs)) return true;
+    const unsigned long long t0 = global_timer_ns();
+    while (true) {
+        if (mbar_try_wait_sleep(bar, parity, kHintNs)) return true;
+        if (global_timer_ns() - t0 > kWaitLimitNs) return false;
+    }
+}
+
 // Programmatic dependent launch.  A kernel launched with
 // cudaLaunchAttributeProgrammaticStreamSerialization may start while the
 // previous kernel of its stream is still running; grid_dep_wait() blocks
@@ -174,6 +201,12 @@ __device__ __forceinline__ void tma_bulk_g2s(void* smem_dst, const void* gsrc, u
         "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(smem_dst)),
         "l"(gsrc), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
+}
+
+// Bulk prefetch of [gsrc, gsrc + bytes) into L2 (no shared memory, no
+// completion to wait for).  16-byte aligned address, size a multiple of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* gsrc, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
 }
 
 template <typename T>

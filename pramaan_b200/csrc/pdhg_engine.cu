@@ -128,6 +128,8 @@ void validate_options(const pramaan_pdhg_options& opt) {
     if (opt.persistent < -1 || opt.persistent > 2) throw InvalidArgument("pdhg options: persistent must be -1, 0, 1 or 2");
     if (opt.gather_cache < -1 || opt.gather_cache > 1) throw InvalidArgument("pdhg options: gather_cache must be -1, 0 or 1");
     if (opt.launch_blocks < 0 || opt.launch_blocks > 64) throw InvalidArgument("pdhg options: launch_blocks must be 0..64");
+    if (opt.panel_split < -1 || opt.panel_split > 1000000)
+        throw InvalidArgument("pdhg options: panel_split must be -1, 0, 1 or a row length up to 1000000");
     if (opt.algorithm == PRAMAAN_ALGO_HALPERN && opt.refine != 1)
         throw InvalidArgument("pdhg options: the Halpern algorithm runs on FP64 master iterates (refine = 1)");
 }
@@ -201,6 +203,9 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     if (opt.algorithm == PRAMAAN_ALGO_ADAPTIVE) setup_adaptive(lp);
     // The step sizes above read the flat operands; interleave them into tile records now.
     if (opt.gather_cache >= 0) select_hot_pair(A_, AT_, dev_, st_);
+    // Reference mode: the long rows of a power-law A go to the column-panel
+    // product (built from the flat operand, so before pack()).
+    if (!adaptive_) build_panel_split(A_, panel_, opt.panel_split, dev_, st_);
     A_.pack(st_);
     AT_.pack(st_);
     // the iteration's vectors: sigma, bounds, y (rows); tau, c, bounds, x, x̄ (columns), plus the gathers
@@ -214,6 +219,7 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     SpmvLauncher<EpiStore<double, double>, double, float, true>::blocks_per_sm(dev_);
     SpmvLauncher<EpiStore<double, double>, double, float, false>::blocks_per_sm(dev_);
     SpmvLauncher<EpiStore<float, float>, float, float, false>::blocks_per_sm(dev_);
+    if (panel_.active) panel_prepare(dev_);
     if (!adaptive_) {
         // The tuner times the fused products of the reference iteration
         // themselves, writing scratch copies of y, x and x̄.
@@ -225,7 +231,9 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
         }
         const EpiDualRef de{sigma_.get(), lr_.get(), ur_.get(), ys.get()};
         const EpiPrimalRef pe{tau_.get(), c_.get(), lx_.get(), ux_.get(), xs.get(), xbs.get()};
-        autotune_operand(A_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
+        // With the panel split the tiled dual product covers the short rows only.
+        autotune_operand(panel_.active ? panel_.S : A_, st_, dev_, status_.get(), opt.gather_cache,
+                         [&](const CsrView& v) {
             SpmvLauncher<EpiDualRef, float, float, false>::launch(v, xbar_.get(), de, status_.get(), st_, dev_);
         }, /*kind=*/1, opt.launch_blocks);
         autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
@@ -292,6 +300,10 @@ void PdhgEngine::launch_dual() {
         return;
     }
     EpiDualRef epi{sigma_.get(), lr_.get(), ur_.get(), y_.get()};
+    if (panel_.active) {
+        panel_launch(panel_, n_, xbar_.get(), epi, status_.get(), st_, dev_);
+        return;
+    }
     SpmvLauncher<EpiDualRef, float, float, false>::launch(A_.view(false), xbar_.get(), epi,
                                                           status_.get(), st_, dev_);
 }
@@ -344,8 +356,10 @@ void PdhgEngine::drain_events() {
         PB_CUDA_CHECK(cudaEventElapsedTime(&ms, ev_pool_[i].a, ev_pool_[i].b));
         if (ev_pool_[i].kind == 0) ms_dual_ += ms; else ms_primal_ += ms;
         // kernels of one product: the main kernel and, when rows cross tiles, their completion
+        // (with the panel split: the panel kernel, the short rows' product, the finish kernel)
         launches_ += ev_pool_[i].kind == 0
-                         ? SpmvLauncher<EpiDualRef, float, float, false>::launches(A_.view(false))
+                         ? (panel_.active ? panel_launches<EpiDualRef>(panel_)
+                                          : SpmvLauncher<EpiDualRef, float, float, false>::launches(A_.view(false)))
                          : SpmvLauncher<EpiPrimalRef, float, float, false>::launches(AT_.view(false));
     }
     ev_used_ = 0;

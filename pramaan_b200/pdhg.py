@@ -136,6 +136,9 @@ class PdhgOptions:
                                 # L1-cached gathers where the autotuner finds them faster;
                                 # 1: L1-cached gathers on every operand without hot slots; -1: plain
     launch_blocks: int = 0      # 0: autotuned blocks per SM of the large-operand products; > 0: fixed
+    panel_split: int = 0        # reference algorithm, A x̄: 0 long rows of a power-law A over column
+                                # panels held in shared memory (automatic), 1 whenever feasible,
+                                # >= 2 with rows of that many entries as long rows, -1 tiled only
 
     def c_struct(self) -> L.COptions:
         o = L.COptions()
@@ -155,6 +158,7 @@ class PdhgOptions:
         o.persistent = int(self.persistent)
         o.gather_cache = int(self.gather_cache)
         o.launch_blocks = int(self.launch_blocks)
+        o.panel_split = int(self.panel_split)
         return o
 
 
@@ -395,6 +399,15 @@ class Session:
         L.check(L.lib().pramaan_session_gather_info(self._h, *(C.byref(q) for q in v)))
         return {"A": {"hot_slots": v[0].value, "l1": bool(v[2].value), "blocks_per_sm": v[4].value},
                 "AT": {"hot_slots": v[1].value, "l1": bool(v[3].value), "blocks_per_sm": v[5].value}}
+
+    def panel_info(self) -> dict:
+        """Column-panel split of the dual product: panels (0: the tiled
+        product alone), long rows, their non-zeros and the row length from
+        which a row is long."""
+        p, lr, ml = C.c_int32(), C.c_int32(), C.c_int32()
+        nz = C.c_int64()
+        L.check(L.lib().pramaan_session_panel_info(self._h, C.byref(p), C.byref(lr), C.byref(nz), C.byref(ml)))
+        return {"panels": p.value, "long_rows": lr.value, "long_nnz": nz.value, "min_len": ml.value}
 
     def gather_slots(self) -> tuple[int, int]:
         """Hot gather slots of A and A^T."""
