@@ -129,7 +129,7 @@ typedef struct pramaan_pdhg_options {
                                  -1: a fixed launch shape, for reproducible
                                  profiles                                       */
     int32_t panel_split;      /* reference algorithm, the A x̄ product:
-                                 0 (default): when rows of at least half the
+                                 0 (default): when rows of at least twice the
                                  panel count of entries hold half or more of
                                  A's non-zeros (power-law row lengths, at
                                  least 4 Mi of them), those long rows are

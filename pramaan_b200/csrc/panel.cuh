@@ -6,7 +6,7 @@
 // per SM per clock (gather_ceiling_kernel, ceiling.cu): the tiled product of
 // a 108 M-entry Zipf LP is bound by that rate at about a third of HBM
 // bandwidth.  The long rows of such an operand hold most of its non-zeros
-// (rows of 74 or more entries hold ~89 % of a Zipf(1.5) LP's), and every one
+// (rows of 296 or more entries hold ~76 % of a Zipf(1.5) LP's), and every one
 // of them touches almost every part of x̄.  So x̄ is cut into P column panels,
 // one per SM, each small enough for shared memory; block p loads panel p of
 // x̄ once per product and streams the entries of all long rows that fall in
@@ -113,7 +113,9 @@ void panel_product_launch(const PanelView& v, const float* x, int* dev_status, c
 
 // Adds the P partials of every long row in panel order and applies the row's
 // epilogue (the same epilogue object as the short rows' tiled product).  One
-// thread per row, 16 partials in flight at a time.
+// thread per row, 8 partials in flight at a time (measured on the 2 M x 5 M
+// Zipf LP: 28 us per launch, against 39 us with 16 predicated loads in flight
+// and 48 us with four threads per row).
 template <class Epi>
 __global__ void __launch_bounds__(256) panel_finish_kernel(const PanelView P, const Epi epi) {
     grid_dep_launch();
@@ -125,14 +127,15 @@ __global__ void __launch_bounds__(256) panel_finish_kernel(const PanelView P, co
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L; r += gridDim.x * blockDim.x) {
         const float* pp = P.part + r;
         float sum = 0.f;
-        for (int q = 0; q < P.panels; q += 16) {
-            float v[16];
+        int q = 0;
+        for (; q + 8 <= P.panels; q += 8) {
+            float v[8];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) v[u] = q + u < P.panels ? __ldcg(pp + size_t(q + u) * ld) : 0.f;
+            for (int u = 0; u < 8; ++u) v[u] = __ldcg(pp + size_t(q + u) * ld);
 #pragma unroll
-            for (int u = 0; u < 16; ++u)
-                if (q + u < P.panels) sum += v[u];
+            for (int u = 0; u < 8; ++u) sum += v[u];
         }
+        for (; q < P.panels; ++q) sum += __ldcg(pp + size_t(q) * ld);
         epi.apply(est, P.long_row[r], sum);
     }
     epi.finish(est, 1);
@@ -160,11 +163,13 @@ struct PanelSplit {
 };
 
 // Default row length from which a row is long: kPanelLenPerPanel x panels.
-// A long row costs 8 P bytes of partials (written and read) plus ~7.2 bytes
-// per entry; a short one a random L2 gather per entry (~4.2 ps at the measured
-// 279 G/s against ~1.1 ps per streamed entry), which breaks even near
-// 0.4 P entries.
-constexpr double kPanelLenPerPanel = 0.5;
+// Every long row costs one segment per panel (its partial written, read back
+// and added by the finish kernel); every short row's entries cost a random L2
+// gather each in the tiled product.  Measured on the 2,000,000 x 5,000,000
+// Zipf LP (148 panels), A x̄ per launch: long from 74 entries 0.360 ms, 110
+// 0.330, 148 0.327, 200 0.320, 260 0.316, 330 0.315, 420 0.322, 550 0.338,
+// 700 0.348.
+constexpr double kPanelLenPerPanel = 2.0;
 // Auto mode takes the split when the long rows hold at least this share of
 // the non-zeros and the operand has at least kPanelMinNnz of them.
 constexpr double kPanelMinShare = 0.5;
