@@ -461,13 +461,16 @@ PRAMAAN_API int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* sl
                                 int32_t* slots_primal, int32_t* l1_dual, int32_t* l1_primal,
                                 int32_t* blocks_dual, int32_t* blocks_primal);
 
-/* Column-panel split of the dual product (option panel_split): the panels
- * (one per SM; 0 when A x̄ runs as the tiled product alone), the long rows
- * they compute, those rows' non-zeros, and the row length from which a row is
- * long.  No reference counterpart (the reference computes A x̄ one thread per
- * row).  Any pointer may be NULL. */
+/* Column-panel split of the products (option panel_split): the panels (one
+ * per SM; 0 when A x̄ runs as the tiled product alone), the long rows they
+ * compute in A x̄, those rows' non-zeros, the row length from which a row is
+ * long, and for Aᵀy the hot rows of A whose y every panel holds and their
+ * non-zeros (0 when Aᵀy runs as the tiled product alone).  No reference
+ * counterpart (the reference computes A x̄ one thread per row and Aᵀy by
+ * atomic scatter).  Any pointer may be NULL. */
 PRAMAAN_API int pramaan_session_panel_info(pramaan_pdhg_session* s, int32_t* panels, int32_t* long_rows,
-                                           int64_t* long_nnz, int32_t* min_len);
+                                           int64_t* long_nnz, int32_t* min_len, int32_t* hot_rows,
+                                           int64_t* hot_nnz);
 
 #ifdef __cplusplus
 }

@@ -120,7 +120,7 @@ SIGNATURES = [
     ("pramaan_session_kernel_bytes", C.c_int, [P, C.POINTER(f64), C.POINTER(f64)]),
     ("pramaan_session_gather_info", C.c_int, [P] + [C.POINTER(i32)] * 6),
     ("pramaan_session_panel_info", C.c_int, [P, C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_int64),
-                                             C.POINTER(i32)]),
+                                             C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_int64)]),
     ("pramaan_release_cached_memory", C.c_int, [i32]),
     ("pramaan_measure_gather_rate", C.c_int, [P, i32, i32, i32, C.POINTER(f64)]),
 ]

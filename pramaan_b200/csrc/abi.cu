@@ -407,16 +407,18 @@ int pramaan_session_gather_info(pramaan_pdhg_session* s, int32_t* slots_dual, in
 }
 
 int pramaan_session_panel_info(pramaan_pdhg_session* s, int32_t* panels, int32_t* long_rows, int64_t* long_nnz,
-                               int32_t* min_len) {
+                               int32_t* min_len, int32_t* hot_rows, int64_t* hot_nnz) {
     return guarded([&] {
         if (!s) throw InvalidArgument("session is NULL");
-        int p = 0, l = 0, ml = 0;
-        long long nz = 0;
-        s->eng->panel_info(&p, &l, &nz, &ml);
+        int p = 0, l = 0, ml = 0, hr = 0;
+        long long nz = 0, hz = 0;
+        s->eng->panel_info(&p, &l, &nz, &ml, &hr, &hz);
         if (panels) *panels = p;
         if (long_rows) *long_rows = l;
         if (long_nnz) *long_nnz = nz;
         if (min_len) *min_len = ml;
+        if (hot_rows) *hot_rows = hr;
+        if (hot_nnz) *hot_nnz = hz;
     });
 }
 

@@ -74,6 +74,22 @@ struct EpiPrimalRef {
     __device__ void finish(State&, int) const {}
 };
 
+// The primal update of a product split in two parts: `add[j]` holds the sum of
+// column j's entries from the hot rows of A (the panel part), and the tiled
+// product over the other entries passes its own sum; Aᵀy = add[j] + sum.
+struct EpiPrimalRefAdd {
+    EpiPrimalRef base;
+    const float* __restrict__ add;
+    using State = NoState;
+    __device__ void init(State&) const {}
+    __device__ void prefetch(int j) const {
+        base.prefetch(j);
+        prefetch_l2(add + j);
+    }
+    __device__ void apply(State& s, int j, float aty) const { base.apply(s, j, __fadd_rn(add[j], aty)); }
+    __device__ void finish(State&, int) const {}
+};
+
 // Reductions land in a small device array of doubles:
 enum ResidSlot : int {
     kSlotRowViol = 0,     // max row violation  (Ax outside [row_lower, row_upper])

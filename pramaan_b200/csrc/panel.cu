@@ -71,20 +71,49 @@ __global__ void __launch_bounds__(kPanelWarps * 32, 1)
     grid_dep_launch();
     grid_dep_wait();
 
-    // ---- panel p of x into shared memory (W is a multiple of 4, x 16-byte aligned) ----
-    const int col0 = p * P.width;
-    int w = P.cols - col0;
-    w = w < 0 ? 0 : (w > P.width ? P.width : w);
-    {
+    // Every thread issues kLoadBatch loads before it stores any, so a block's
+    // start costs a few L2 round trips rather than one per loop pass.
+    constexpr int kLoadBatch = 8;
+    const int nthr = blockDim.x;
+    if (P.vec_idx) {
+        // ---- the gathered entries of x (the same for every block) ----
+        const int V = P.vec_len;
+        for (int k0 = threadIdx.x; k0 < V; k0 += nthr * kLoadBatch) {
+            int idx[kLoadBatch];
+            float v[kLoadBatch];
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; ++u) {
+                const int k = k0 + u * nthr;
+                idx[u] = k < V ? __ldg(P.vec_idx + k) : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; ++u) v[u] = k0 + u * nthr < V ? __ldcg(x + idx[u]) : 0.f;
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; ++u)
+                if (k0 + u * nthr < V) xs[k0 + u * nthr] = v[u];
+        }
+    } else {
+        // ---- panel p of x (W is a multiple of 4, x 16-byte aligned) ----
+        const int col0 = p * P.width;
+        int w = P.cols - col0;
+        w = w < 0 ? 0 : (w > P.width ? P.width : w);
         const int w4 = w >> 2;
         const float4* x4 = reinterpret_cast<const float4*>(x + col0);
         float4* xs4 = reinterpret_cast<float4*>(xs);
-        for (int k = threadIdx.x; k < w4; k += blockDim.x) xs4[k] = __ldcg(x4 + k);
-        for (int k = (w4 << 2) + threadIdx.x; k < w; k += blockDim.x) xs[k] = __ldcg(x + col0 + k);
+        for (int k0 = threadIdx.x; k0 < w4; k0 += nthr * kLoadBatch) {
+            float4 v[kLoadBatch];
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; ++u)
+                v[u] = k0 + u * nthr < w4 ? __ldcg(x4 + k0 + u * nthr) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; ++u)
+                if (k0 + u * nthr < w4) xs4[k0 + u * nthr] = v[u];
+        }
+        for (int k = (w4 << 2) + threadIdx.x; k < w; k += nthr) xs[k] = __ldcg(x + col0 + k);
     }
     __syncthreads();
 
-    float* out_panel = P.part + size_t(p) * size_t(P.long_rows);
+    float* out_panel = P.part + size_t(p) * size_t(P.out_stride);
     bool failed = false;
     int i = 0;
     for (; i < mine; ++i) {
@@ -308,7 +337,7 @@ __global__ void __launch_bounds__(256) fill_kernel(const int4* __restrict__ desc
             unsigned short cc = 0;
             float vv = 0.f;
             if (q < nent) {
-                const int src = perm[d.z + q];
+                const int src = perm ? perm[d.z + q] : d.z + q;
                 cc = lcol[src];
                 vv = lval[src];
             }
@@ -326,15 +355,19 @@ __global__ void __launch_bounds__(256) fill_kernel(const int4* __restrict__ desc
 // Checks every record once after it is built, so that the panel kernel can
 // trust them without per-access clamps: segment count and offsets within the
 // record, its segments within the long rows, every column inside its panel.
+// vec_len > 0: every gather index must lie below vec_len (hot part of Aᵀy);
+// else inside the record's panel of the columns.
 __global__ void __launch_bounds__(256) check_records_kernel(const unsigned char* __restrict__ rec,
                                                             const int4* __restrict__ desc, int nchunks, int L,
-                                                            int width, int cols, int* __restrict__ bad) {
+                                                            int width, int cols, int vec_len,
+                                                            int* __restrict__ bad) {
     for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const unsigned char* R = rec + size_t(c) * PanelRec::bytes;
         const int4 h = *reinterpret_cast<const int4*>(R + PanelRec::off_head);
         const int p = desc[c].w;
         int w = cols - p * width;
         w = w > width ? width : w;
+        if (vec_len > 0) w = vec_len;
         const bool head_ok = h.y >= 0 && h.y <= kPanelSegCap && h.x >= 0 && h.x + h.y <= L && w > 0;
         if (!head_ok) {
             if (threadIdx.x == 0) atomicOr(bad, 1);
@@ -383,9 +416,9 @@ void panel_prepare(int dev) {
 }
 
 void panel_product_launch(const PanelView& v, const float* x, int* dev_status, cudaStream_t st) {
-    if (v.panels <= 0 || v.long_rows <= 0) return;
-    launch_dependent(&panel_product_kernel, v.panels, kPanelWarps * 32, PanelSmem::bytes(v.width), st, v, x,
-                     dev_status);
+    if (v.panels <= 0 || v.out_stride <= 0) return;
+    launch_dependent(&panel_product_kernel, v.panels, kPanelWarps * 32,
+                     PanelSmem::bytes(v.vec_idx ? v.vec_len : v.width), st, v, x, dev_status);
 }
 
 void build_panel_split(const CsrDevice& A, PanelSplit& ps, int mode, int dev, cudaStream_t st) {
@@ -478,7 +511,7 @@ void build_panel_split(const CsrDevice& A, PanelSplit& ps, int mode, int dev, cu
         DevBuf<int> bad(1);
         PB_CUDA_CHECK(cudaMemsetAsync(bad.get(), 0, 4, st));
         check_records_kernel<<<std::min(nchunks, 65535 * 8), 256, 0, st>>>(ps.rec.get(), desc.get(), nchunks, L,
-                                                                          width, cols, bad.get());
+                                                                          width, cols, 0, bad.get());
         PB_CUDA_CHECK(cudaGetLastError());
         if (read_one(bad.get(), st)) throw std::logic_error("build_panel_split: a panel record failed its check");
     }
@@ -525,6 +558,196 @@ void build_panel_split(const CsrDevice& A, PanelSplit& ps, int mode, int dev, cu
     ps.min_len = thr;
     ps.num_chunks = nchunks;
     ps.long_nnz = nl;
+}
+
+// ---------------------------------------------------------------------------
+// Hot part of Aᵀy: the longest rows of A, per column panel
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void row_len_kernel(const int* __restrict__ rp, int rows, int* __restrict__ len) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x)
+        len[i] = rp[i + 1] - rp[i];
+}
+
+// Rows of at least `thr` entries are hot (flag 1, plus a trailing 0 for the
+// scan); `rest_len` is a row's length in the remaining operand (0 when hot).
+__global__ void hot_rows_kernel(const int* __restrict__ rp, int rows, int thr, int* __restrict__ hot,
+                                int* __restrict__ rest_len) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= rows; i += gridDim.x * blockDim.x) {
+        const int len = i < rows ? rp[i + 1] - rp[i] : 0;
+        const bool h = i < rows && len >= thr;
+        hot[i] = h ? 1 : 0;
+        rest_len[i] = h ? 0 : len;
+    }
+}
+
+// Per column j of A (row of Aᵀ): entries from hot rows and from the others,
+// padded with zeros to `padded` columns (+1 for the scans).
+__global__ void split_counts_kernel(const int* __restrict__ trp, const int* __restrict__ trow, int cols,
+                                    int padded, const int* __restrict__ hot, int* __restrict__ nh,
+                                    int* __restrict__ nr) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= padded; j += gridDim.x * blockDim.x) {
+        int h = 0, r = 0;
+        if (j < cols) {
+            for (int k = trp[j]; k < trp[j + 1]; ++k) {
+                if (hot[trow[k]]) ++h; else ++r;
+            }
+        }
+        nh[j] = h;
+        nr[j] = r;
+    }
+}
+
+// Copies Aᵀ's entries of hot rows (index among the hot rows, value) and of
+// the other rows (the remaining operand), keeping Aᵀ's order.
+__global__ void split_copy_kernel(const int* __restrict__ trp, const int* __restrict__ trow,
+                                  const float* __restrict__ tval, int cols, const int* __restrict__ hot,
+                                  const int* __restrict__ hidx, const int* __restrict__ hoff,
+                                  const int* __restrict__ roff, unsigned short* __restrict__ hcol,
+                                  float* __restrict__ hval, int* __restrict__ rcol, float* __restrict__ rval) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cols; j += gridDim.x * blockDim.x) {
+        int h = hoff[j], r = roff[j];
+        for (int k = trp[j]; k < trp[j + 1]; ++k) {
+            const int i = trow[k];
+            if (hot[i]) {
+                hcol[h] = static_cast<unsigned short>(hidx[i]);
+                hval[h] = tval[k];
+                ++h;
+            } else {
+                rcol[r] = i;
+                rval[r] = tval[k];
+                ++r;
+            }
+        }
+    }
+}
+
+__global__ void hot_list_kernel(const int* __restrict__ hot, const int* __restrict__ hidx, int rows,
+                                int* __restrict__ list) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x)
+        if (hot[i]) list[hidx[i]] = i;
+}
+
+__global__ void max_kernel(const int* __restrict__ a, long long n, int* __restrict__ out) {
+    int m = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = max(m, a[i]);
+    atomicMax(out, m);
+}
+
+}  // namespace
+
+void build_panel_hot(const CsrDevice& A, const CsrDevice& AT, const PanelSplit& dual, PanelHot& ph, int gather_cache,
+                     int dev, cudaStream_t st) {
+    ph = PanelHot{};
+    if (!dual.active) return;
+    const int rows = A.rows, cols = A.cols;
+    if (AT.packed || !AT.col.get() || !AT.val.get()) throw std::logic_error("build_panel_hot needs the flat transpose");
+    const size_t limit = panel_smem_limit(dev);
+    if (limit <= PanelSmem::off_x) return;
+    const int vmax = std::min<long long>((limit - PanelSmem::off_x) / 4, 65536);
+    const int panels = dual.panels, width = dual.width;
+    const long long padded = (long long)panels * width;
+    if (padded + 1 > INT_MAX) return;
+
+    // ---- the hot rows: the vmax longest (ties at the cut left out), at least kPanelHotMinLen long ----
+    DevBuf<int> len{size_t(rows)}, len_sorted{size_t(rows)};
+    row_len_kernel<<<grid_for_n(rows), kThreads, 0, st>>>(A.row_ptr.get(), rows, len.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    {
+        size_t tb = 0;
+        PB_CUDA_CHECK(cub::DeviceRadixSort::SortKeysDescending(nullptr, tb, len.get(), len_sorted.get(), rows, 0, 32, st));
+        DevBuf<unsigned char> temp(tb > 0 ? tb : 1);
+        PB_CUDA_CHECK(cub::DeviceRadixSort::SortKeysDescending(temp.get(), tb, len.get(), len_sorted.get(), rows, 0,
+                                                               32, st));
+        PB_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    int thr = kPanelHotMinLen;
+    if (rows > vmax) thr = std::max(thr, read_one(len_sorted.get() + vmax, st) + 1);
+    len.reset();
+    len_sorted.reset();
+    DevBuf<int> hot{size_t(rows) + 1}, hidx{size_t(rows) + 1}, rest_len{size_t(rows) + 1}, rest_rp{size_t(rows) + 1};
+    hot_rows_kernel<<<grid_for_n(rows + 1LL), kThreads, 0, st>>>(A.row_ptr.get(), rows, thr, hot.get(),
+                                                                  rest_len.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    exclusive_sum(hot.get(), hidx.get(), rows + 1LL, st);
+    exclusive_sum(rest_len.get(), rest_rp.get(), rows + 1LL, st);
+    const int V = read_one(hidx.get() + rows, st);
+    if (V <= 0 || V > vmax) return;
+
+    // ---- Aᵀ's entries split by row: hot (per column, in Aᵀ order) and the rest ----
+    DevBuf<int> nh{size_t(padded) + 1}, nr{size_t(padded) + 1}, hoff{size_t(padded) + 1}, roff{size_t(padded) + 1};
+    split_counts_kernel<<<grid_for_n(padded + 1), kThreads, 0, st>>>(AT.row_ptr.get(), AT.col.get(), cols,
+                                                                      int(padded), hot.get(), nh.get(), nr.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    {
+        DevBuf<int> longest(1);
+        PB_CUDA_CHECK(cudaMemsetAsync(longest.get(), 0, 4, st));
+        max_kernel<<<grid_for_n(padded), kThreads, 0, st>>>(nh.get(), padded, longest.get());
+        PB_CUDA_CHECK(cudaGetLastError());
+        if (read_one(longest.get(), st) > kPanelEnt) return;   // a column with more hot entries than a chunk
+    }
+    exclusive_sum(nh.get(), hoff.get(), padded + 1, st);
+    exclusive_sum(nr.get(), roff.get(), padded + 1, st);
+    const int nhot = read_one(hoff.get() + padded, st);
+    const int nrest = read_one(roff.get() + padded, st);
+    if (nhot <= 0) return;
+    DevBuf<unsigned short> hcol{size_t(nhot)};
+    DevBuf<float> hval{size_t(nhot)};
+    CsrDevice& R = ph.rest;
+    R.allocate(cols, rows, nrest, /*lo=*/false);
+    PB_CUDA_CHECK(cudaMemcpyAsync(R.row_ptr.get(), roff.get(), (size_t(cols) + 1) * 4, cudaMemcpyDeviceToDevice, st));
+    split_copy_kernel<<<grid_for_n(cols), kThreads, 0, st>>>(AT.row_ptr.get(), AT.col.get(), AT.val.get(), cols,
+                                                            hot.get(), hidx.get(), hoff.get(), roff.get(), hcol.get(),
+                                                            hval.get(), R.col.get(), R.val.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+
+    // ---- chunks of every panel's columns (segments: the panel's W columns) ----
+    DevBuf<int> nch{size_t(panels) + 1};
+    PB_CUDA_CHECK(cudaMemsetAsync(nch.get(), 0, nch.bytes(), st));
+    chunk_kernel<<<(panels + 63) / 64, 64, 0, st>>>(nh.get(), hoff.get(), width, panels, nch.get(), nullptr,
+                                                    nullptr);
+    PB_CUDA_CHECK(cudaGetLastError());
+    ph.chunk_ptr.alloc(size_t(panels) + 1);
+    exclusive_sum(nch.get(), ph.chunk_ptr.get(), panels + 1LL, st);
+    const int nchunks = read_one(ph.chunk_ptr.get() + panels, st);
+    DevBuf<int4> desc{size_t(nchunks > 0 ? nchunks : 1)};
+    chunk_kernel<<<(panels + 63) / 64, 64, 0, st>>>(nh.get(), hoff.get(), width, panels, nullptr,
+                                                    ph.chunk_ptr.get(), desc.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    ph.rec.alloc(size_t(nchunks) * PanelRec::bytes);
+    PB_CUDA_CHECK(cudaMemsetAsync(ph.rec.get(), 0, ph.rec.bytes(), st));
+    fill_kernel<<<std::min(nchunks, 65535 * 8), 256, 0, st>>>(desc.get(), nchunks, nh.get(), hoff.get(), width,
+                                                             nullptr, hcol.get(), hval.get(), ph.rec.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    {
+        DevBuf<int> bad(1);
+        PB_CUDA_CHECK(cudaMemsetAsync(bad.get(), 0, 4, st));
+        check_records_kernel<<<std::min(nchunks, 65535 * 8), 256, 0, st>>>(ph.rec.get(), desc.get(), nchunks,
+                                                                          width, width, cols, V, bad.get());
+        PB_CUDA_CHECK(cudaGetLastError());
+        if (read_one(bad.get(), st)) throw std::logic_error("build_panel_hot: a panel record failed its check");
+    }
+    ph.hot_row.alloc(size_t(V));
+    hot_list_kernel<<<grid_for_n(rows), kThreads, 0, st>>>(hot.get(), hidx.get(), rows, ph.hot_row.get());
+    PB_CUDA_CHECK(cudaGetLastError());
+    ph.part.alloc(size_t(padded));
+    PB_CUDA_CHECK(cudaMemsetAsync(ph.part.get(), 0, ph.part.bytes(), st));
+
+    // ---- the remaining operand: hot gather slots among the other rows, then tile records ----
+    R.finalize(st);
+    if (gather_cache >= 0) R.select_hot(rest_rp.get(), rows, dev, st);
+    R.pack(st);
+    PB_CUDA_CHECK(cudaStreamSynchronize(st));   // temporaries are freed on return
+
+    ph.active = true;
+    ph.panels = panels;
+    ph.width = width;
+    ph.hot_rows = V;
+    ph.min_len = thr;
+    ph.num_chunks = nchunks;
+    ph.hot_nnz = nhot;
 }
 
 }  // namespace pb

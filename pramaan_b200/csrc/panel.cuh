@@ -85,15 +85,26 @@ static_assert(panel_val_slot(0) == 0 && panel_val_slot(4) == 128 && panel_val_sl
               "panel_val_slot layout");
 
 // Device view of one operand's panel split.
+// The same kernel serves two layouts:
+//   * the A x̄ split (vec_idx null): block p gathers from x̄[p W, p W + W),
+//     its segments are the long rows, and segment s of panel p is written to
+//     part[p * L + s];
+//   * the hot part of Aᵀy (vec_idx set): every block gathers from the
+//     vec_len entries x[vec_idx[k]] (y of the longest rows of A), its
+//     segments are the W columns of its panel, and segment s of panel p is
+//     written to part[p * W + s] (the column itself).
 struct PanelView {
     int panels = 0;       // P (one block each)
     int width = 0;        // columns per panel W (a multiple of 4)
     int cols = 0;         // columns of the operand
-    int long_rows = 0;    // L
+    int long_rows = 0;    // L (A x̄ split) or 0
     const unsigned char* rec = nullptr;   // chunk records, panel-major
     const int* chunk_ptr = nullptr;       // [P + 1]
     const int* long_row = nullptr;        // [L] original row of every long row
-    float* part = nullptr;                // [P * L] per-panel partial sums
+    float* part = nullptr;                // [P * out_stride] per-panel sums
+    int out_stride = 0;                   // L or W
+    const int* vec_idx = nullptr;         // [vec_len] gathered vector entries (hot part of Aᵀy)
+    int vec_len = 0;
 };
 
 // Shared memory of the panel kernel: the warps' rings, their mbarriers, then
@@ -155,6 +166,7 @@ struct PanelSplit {
         PanelView v;
         v.panels = panels; v.width = width; v.cols = cols; v.long_rows = long_rows;
         v.rec = rec.get(); v.chunk_ptr = chunk_ptr.get(); v.long_row = long_row.get(); v.part = part.get();
+        v.out_stride = long_rows;
         return v;
     }
     size_t device_bytes() const {
@@ -174,6 +186,43 @@ constexpr double kPanelLenPerPanel = 2.0;
 // the non-zeros and the operand has at least kPanelMinNnz of them.
 constexpr double kPanelMinShare = 0.5;
 constexpr long long kPanelMinNnz = 4LL << 20;
+
+// The hot part of Aᵀy.  The rows of A whose y entries every column gathers
+// most are the longest rows; their y entries fit in one block's shared memory
+// (up to PanelSmem::max_width of them).  Block p holds those entries of y and
+// streams, for the columns of its panel (the same panels as the A x̄ split),
+// the hot rows' entries in column order: segment s of panel p is column
+// p W + s, and part[p W + s] receives its sum over the hot rows.  The other
+// entries of Aᵀ form the remaining operand, whose tiled product adds part[j]
+// to its own sum in the primal update (EpiPrimalRefAdd).
+struct PanelHot {
+    bool active = false;
+    int panels = 0, width = 0, hot_rows = 0, min_len = 0, num_chunks = 0;
+    long long hot_nnz = 0;
+    CsrDevice rest;                     // Aᵀ without the hot rows' entries
+    DevBuf<unsigned char> rec;
+    DevBuf<int> chunk_ptr, hot_row;
+    DevBuf<float> part;                 // [P W]: per column, the sum over the hot rows
+    PanelView view(int cols) const {
+        PanelView v;
+        v.panels = panels; v.width = width; v.cols = cols;
+        v.rec = rec.get(); v.chunk_ptr = chunk_ptr.get(); v.part = part.get();
+        v.out_stride = width;
+        v.vec_idx = hot_row.get();
+        v.vec_len = hot_rows;
+        return v;
+    }
+};
+// Rows shorter than this never count as hot rows of Aᵀy.
+constexpr int kPanelHotMinLen = 32;
+
+// Builds the hot part of Aᵀy for an operand whose A x̄ is split (`dual`
+// active), from the flat A and Aᵀ (before pack()).  Leaves ph inactive when
+// no row qualifies or a column has more hot entries than a chunk holds.  The
+// remaining operand gets hot gather slots as any operand does (none with
+// gather_cache -1).  Synchronises `st`.
+void build_panel_hot(const CsrDevice& A, const CsrDevice& AT, const PanelSplit& dual, PanelHot& ph, int gather_cache,
+                     int dev, cudaStream_t st);
 
 // Builds the split of A (flat arrays, before A.pack()).  mode 0: automatic
 // (power-law operands only); 1: whenever feasible, long rows from the default

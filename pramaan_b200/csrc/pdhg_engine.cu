@@ -205,7 +205,10 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     if (opt.gather_cache >= 0) select_hot_pair(A_, AT_, dev_, st_);
     // Reference mode: the long rows of a power-law A go to the column-panel
     // product (built from the flat operand, so before pack()).
-    if (!adaptive_) build_panel_split(A_, panel_, opt.panel_split, dev_, st_);
+    if (!adaptive_) {
+        build_panel_split(A_, panel_, opt.panel_split, dev_, st_);
+        build_panel_hot(A_, AT_, panel_, panel_t_, opt.gather_cache, dev_, st_);
+    }
     A_.pack(st_);
     AT_.pack(st_);
     // the iteration's vectors: sigma, bounds, y (rows); tau, c, bounds, x, x̄ (columns), plus the gathers
@@ -219,6 +222,7 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
     SpmvLauncher<EpiStore<double, double>, double, float, true>::blocks_per_sm(dev_);
     SpmvLauncher<EpiStore<double, double>, double, float, false>::blocks_per_sm(dev_);
     SpmvLauncher<EpiStore<float, float>, float, float, false>::blocks_per_sm(dev_);
+    SpmvLauncher<EpiPrimalRefAdd, float, float, false>::blocks_per_sm(dev_);
     if (panel_.active) panel_prepare(dev_);
     if (!adaptive_) {
         // The tuner times the fused products of the reference iteration
@@ -236,9 +240,17 @@ PdhgEngine::PdhgEngine(const pramaan_lp& lp, const pramaan_pdhg_options& opt) : 
                          [&](const CsrView& v) {
             SpmvLauncher<EpiDualRef, float, float, false>::launch(v, xbar_.get(), de, status_.get(), st_, dev_);
         }, /*kind=*/1, opt.launch_blocks);
-        autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
-            SpmvLauncher<EpiPrimalRef, float, float, false>::launch(v, y_.get(), pe, status_.get(), st_, dev_);
-        }, /*kind=*/2, opt.launch_blocks);
+        if (panel_t_.active) {
+            // the tiled primal product covers the entries outside the hot rows
+            const EpiPrimalRefAdd pa{pe, panel_t_.part.get()};
+            autotune_operand(panel_t_.rest, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
+                SpmvLauncher<EpiPrimalRefAdd, float, float, false>::launch(v, y_.get(), pa, status_.get(), st_, dev_);
+            }, /*kind=*/5, opt.launch_blocks);
+        } else {
+            autotune_operand(AT_, st_, dev_, status_.get(), opt.gather_cache, [&](const CsrView& v) {
+                SpmvLauncher<EpiPrimalRef, float, float, false>::launch(v, y_.get(), pe, status_.get(), st_, dev_);
+            }, /*kind=*/2, opt.launch_blocks);
+        }
         PB_CUDA_CHECK(cudaStreamSynchronize(st_));   // scratch copies are freed on return
     } else {
         // The FP32 product kernels share one shared-memory layout, so the grid the
@@ -318,6 +330,15 @@ void PdhgEngine::launch_primal() {
         return;
     }
     EpiPrimalRef epi{tau_.get(), c_.get(), lx_.get(), ux_.get(), x_.get(), xbar_.get()};
+    if (panel_t_.active) {
+        // the hot rows' part per column (panel kernel), then the other entries
+        // with the primal update adding that part
+        panel_product_launch(panel_t_.view(n_), y_.get(), status_.get(), st_);
+        const EpiPrimalRefAdd pa{epi, panel_t_.part.get()};
+        SpmvLauncher<EpiPrimalRefAdd, float, float, false>::launch(panel_t_.rest.view(false), y_.get(), pa,
+                                                                   status_.get(), st_, dev_);
+        return;
+    }
     SpmvLauncher<EpiPrimalRef, float, float, false>::launch(AT_.view(false), y_.get(), epi,
                                                             status_.get(), st_, dev_);
 }
@@ -360,7 +381,9 @@ void PdhgEngine::drain_events() {
         launches_ += ev_pool_[i].kind == 0
                          ? (panel_.active ? panel_launches<EpiDualRef>(panel_)
                                           : SpmvLauncher<EpiDualRef, float, float, false>::launches(A_.view(false)))
-                         : SpmvLauncher<EpiPrimalRef, float, float, false>::launches(AT_.view(false));
+                         : (panel_t_.active
+                                ? 1 + SpmvLauncher<EpiPrimalRefAdd, float, float, false>::launches(panel_t_.rest.view(false))
+                                : SpmvLauncher<EpiPrimalRef, float, float, false>::launches(AT_.view(false)));
     }
     ev_used_ = 0;
 }

@@ -52,20 +52,26 @@ public:
     double bytes_dual() const;
     double bytes_primal() const;
     int hot_slots_dual() const { return A_.hot; }
-    int hot_slots_primal() const { return AT_.hot; }
+    // the tiled primal product's operand: the remaining entries when Aᵀy is split
+    int hot_slots_primal() const { return panel_t_.active ? panel_t_.rest.hot : AT_.hot; }
     // the tiled dual product's operand: the short rows when A x̄ is split over panels
     int gather_l1_dual() const { return panel_.active ? panel_.S.gather_l1 : A_.gather_l1; }
-    int gather_l1_primal() const { return AT_.gather_l1; }
+    int gather_l1_primal() const { return panel_t_.active ? panel_t_.rest.gather_l1 : AT_.gather_l1; }
     int blocks_dual() const { return panel_.active ? panel_.S.tuned_blocks_per_sm : A_.tuned_blocks_per_sm; }
     // Column-panel split of the A x̄ product (reference mode): panels, long rows
     // and their non-zeros, the row length from which a row is long (0: not split).
-    void panel_info(int* panels, int* long_rows, long long* long_nnz, int* min_len) const {
+    // The hot part of Aᵀy: the rows of A whose y every block holds, their
+    // non-zeros (0: the tiled product alone).
+    void panel_info(int* panels, int* long_rows, long long* long_nnz, int* min_len, int* hot_rows,
+                    long long* hot_nnz) const {
         *panels = panel_.active ? panel_.panels : 0;
         *long_rows = panel_.active ? panel_.long_rows : 0;
         *long_nnz = panel_.active ? panel_.long_nnz : 0;
         *min_len = panel_.active ? panel_.min_len : 0;
+        *hot_rows = panel_t_.active ? panel_t_.hot_rows : 0;
+        *hot_nnz = panel_t_.active ? panel_t_.hot_nnz : 0;
     }
-    int blocks_primal() const { return AT_.tuned_blocks_per_sm; }
+    int blocks_primal() const { return panel_t_.active ? panel_t_.rest.tuned_blocks_per_sm : AT_.tuned_blocks_per_sm; }
     void synchronize();
 
     // ---- adaptive mode (pdhg_adaptive.cu) ----
@@ -115,6 +121,7 @@ private:
 
     CsrDevice A_, AT_;
     PanelSplit panel_;   // A x̄ over column panels (reference mode, power-law operands)
+    PanelHot panel_t_;   // the longest rows' part of Aᵀy over the same panels
     DevBuf<float> c_, lr_, ur_, lx_, ux_, sigma_, tau_, x_, y_, xbar_;
     DevBuf<double> rlo64_, rhi64_, vlo64_, vhi64_, slots_;
     DevBuf<int> status_;

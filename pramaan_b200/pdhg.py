@@ -401,13 +401,16 @@ class Session:
                 "AT": {"hot_slots": v[1].value, "l1": bool(v[3].value), "blocks_per_sm": v[5].value}}
 
     def panel_info(self) -> dict:
-        """Column-panel split of the dual product: panels (0: the tiled
-        product alone), long rows, their non-zeros and the row length from
-        which a row is long."""
-        p, lr, ml = C.c_int32(), C.c_int32(), C.c_int32()
-        nz = C.c_int64()
-        L.check(L.lib().pramaan_session_panel_info(self._h, C.byref(p), C.byref(lr), C.byref(nz), C.byref(ml)))
-        return {"panels": p.value, "long_rows": lr.value, "long_nnz": nz.value, "min_len": ml.value}
+        """Column-panel split of the products: panels (0: the tiled A x̄
+        alone), long rows of A x̄, their non-zeros and the row length from
+        which a row is long; the hot rows of Aᵀy (0: the tiled Aᵀy alone)
+        and their non-zeros."""
+        p, lr, ml, hr = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        nz, hz = C.c_int64(), C.c_int64()
+        L.check(L.lib().pramaan_session_panel_info(self._h, C.byref(p), C.byref(lr), C.byref(nz), C.byref(ml),
+                                                   C.byref(hr), C.byref(hz)))
+        return {"panels": p.value, "long_rows": lr.value, "long_nnz": nz.value, "min_len": ml.value,
+                "primal_hot_rows": hr.value, "primal_hot_nnz": hz.value}
 
     def gather_slots(self) -> tuple[int, int]:
         """Hot gather slots of A and A^T."""

@@ -3,6 +3,9 @@
 On an LP with power-law row lengths the transpose's gathers concentrate on
 the long rows' y entries; the products keep those entries in shared memory.
 Operands with local columns may instead have their gathers cached in L1.
+The reference-mode cases run with the column-panel split off (panel_split
+-1): they test the tiled kernels' gather modes, which the split would take
+the longest rows away from (the split has its own tests, test_gpu_panel.py).
 The value gathered is the same in every mode, so every iterate must be
 bit-identical with the option gather_cache at 0 (automatic), 1 (L1-cached
 gathers wherever there are no hot slots) and -1 (plain L2 gathers), in the
@@ -31,7 +34,7 @@ def zipf_mid():
 def test_reference_iterates_identical_with_and_without_cache(zipf_mid):
     runs = {}
     for cache in (0, -1):
-        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE, panel_split=-1,
                         gather_cache=cache)
         with Session(zipf_mid, o) as s:
             slots = s.gather_slots()
@@ -77,7 +80,7 @@ def banded_mid():
 def test_l1_cached_gathers_identical_to_l2_gathers(banded_mid):
     runs = {}
     for cache in (1, 0, -1):
-        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE, panel_split=-1,
                         gather_cache=cache)
         with Session(banded_mid, o) as s:
             info = s.gather_info()
@@ -124,7 +127,7 @@ def test_hot_slots_with_row_maps_identical(zipf_mid):
     md = _with_empty_rows_and_columns(zipf_mid)
     runs = {}
     for cache in (0, 1, -1):
-        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+        o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE, panel_split=-1,
                         gather_cache=cache)
         with Session(md, o) as s:
             info = s.gather_info()
@@ -154,7 +157,7 @@ def test_launch_shape_changes_no_iterate(blocks):
     for cache in (1, -1):
         runs = []
         for lb in (0, blocks):
-            o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE,
+            o = PdhgOptions(tolerance=1e-12, max_iterations=1000, check_frequency=100, algorithm=ALGO_REFERENCE, panel_split=-1,
                             gather_cache=cache, launch_blocks=lb)
             with Session(md, o) as s:
                 s.iterate(40)

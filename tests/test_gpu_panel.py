@@ -1,9 +1,11 @@
-"""Column-panel split of the A x̄ product (csrc/panel.cuh, panel.cu).
+"""Column-panel split of the products (csrc/panel.cuh, panel.cu).
 
 The long rows of A are computed over column panels of x̄ held in shared
 memory (one per SM) and their per-panel partial sums added in panel order;
-the short rows keep the tiled product.  The split changes only the order of
-the additions within a long row, so:
+the short rows keep the tiled product.  The longest rows' part of Aᵀy runs
+over the same panels (every block holds those rows' y, one segment per
+column) and the tiled Aᵀy over the other entries adds it.  The splits change
+only the order of the additions, so:
   * iterates after k reference iterations match the oracle's restatement of
     the reference iteration (src/gpu/pdhg_kernels.cuh:24-109) within
     |gpu - ref| <= 1e-4 * (1 + |ref|), the tolerance of the tiled product's
@@ -71,6 +73,8 @@ def test_panel_trajectory_matches_oracle(zipf_small, k):
     info, x, y = _run(zipf_small, k, 1)
     assert info["panels"] > 100 and info["long_rows"] > 0
     assert info["long_nnz"] > 0.5 * zipf_small.nnz()
+    # the longest rows' part of A^T y runs over the same panels
+    assert info["primal_hot_rows"] > 0 and info["primal_hot_nnz"] > 0.5 * zipf_small.nnz()
     _check_oracle(zipf_small, k, x, y, "zipf 20k x 300k")
 
 
@@ -79,7 +83,7 @@ def test_panel_deterministic_and_matches_tiled(zipf_small):
     _, x2, y2 = _run(zipf_small, 30, 1)
     assert np.array_equal(x1, x2) and np.array_equal(y1, y2)
     info, xt, yt = _run(zipf_small, 30, -1)
-    assert info["panels"] == 0
+    assert info["panels"] == 0 and info["primal_hot_rows"] == 0
     np.testing.assert_allclose(x1, xt, rtol=1e-4, atol=1e-4)
     np.testing.assert_allclose(y1, yt, rtol=1e-4, atol=1e-4 * (1 + np.abs(yt).max()))
 
@@ -97,6 +101,7 @@ def test_panel_long_row_sets(min_len):
     model = _mixed_lp(11)
     info, x, y = _run(model, 12, min_len)
     assert info["panels"] > 0 and info["min_len"] == min_len
+    assert info["primal_hot_rows"] == int((np.diff(model.row_ptr) >= 32).sum())   # rows of >= 32 entries
     lens = np.diff(model.row_ptr)
     assert info["long_rows"] == int((lens >= min_len).sum())
     _check_oracle(model, 12, x, y, f"mixed, long rows >= {min_len}")
@@ -110,6 +115,8 @@ def test_panel_narrow_panels():
     model = _feasible(rp, ci, v, m, n, 3)
     info, x, y = _run(model, 15, 2)
     assert 0 < info["panels"] <= 100
+    # about 400 hot entries per column: more than a chunk, so A^T y stays tiled
+    assert info["primal_hot_rows"] == 0
     _check_oracle(model, 15, x, y, "narrow panels")
 
 
