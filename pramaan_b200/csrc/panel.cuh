@@ -169,9 +169,6 @@ struct PanelSplit {
         v.out_stride = long_rows;
         return v;
     }
-    size_t device_bytes() const {
-        return S.device_bytes() + rec.bytes() + chunk_ptr.bytes() + long_row.bytes() + part.bytes();
-    }
 };
 
 // Default row length from which a row is long: kPanelLenPerPanel x panels.

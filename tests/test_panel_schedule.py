@@ -9,7 +9,9 @@ piece per lane it touches, the finish as the sum over panels in order).
 On random structures — empty rows, rows crossing every panel, rows shorter
 than the threshold, narrow panels, chunks closed by the segment cap — every
 long row must receive exactly the sum of its entries and every short row
-must be left to the tiled product.  Products are small integers, so the sums
+must be left to the tiled product.  The same records and arithmetic, laid out
+for the hot part of Aᵀy (the longest rows of A, one segment per column of a
+panel), plus the tiled rest must give every column of Aᵀy exactly.  Products are small integers, so the sums
 are exact whatever the order.
 """
 import numpy as np
@@ -150,3 +152,111 @@ def test_segment_cap_closes_chunks():
         mine = [r for r in records if r[0] == p]
         assert len(mine) == -(-m // SEG_CAP)
         assert all(len(r[2]) == SEG_CAP for r in mine[:-1])
+
+
+# ---------------------------------------------------------------------------
+# The hot part of Aᵀy (build_panel_hot): the longest rows of A, their y held by
+# every block, one segment per column of the block's panel in column order.
+# ---------------------------------------------------------------------------
+
+HOT_MIN_LEN = 32
+
+
+def chunk_segments(segs):
+    """Greedy chunking of one panel's segments (lists of entries)."""
+    out, r = [], 0
+    while r < len(segs):
+        first, ent = r, 0
+        while r < len(segs) and r - first < SEG_CAP and ent + len(segs[r]) <= ENT:
+            ent += len(segs[r])
+            r += 1
+        out.append((first, segs[first:r]))
+    return out
+
+
+def run_records(records, vec, nseg):
+    """The kernel's arithmetic over (first, [[(gather index, value), ...], ...])
+    records: in-lane segmented prefixes, pieces per lane, segment sums."""
+    out = np.full(nseg, np.nan)
+    for first, segs in records:
+        entries = [e for s in segs for e in s]
+        nent = len(entries)
+        off = np.zeros(len(segs) + 1, np.int64)
+        off[1:] = np.cumsum([len(s) for s in segs])
+        starts = np.zeros(ENT + 1, bool)
+        for a, b in zip(off[:-1], off[1:]):
+            if a < b:
+                starts[a] = True
+        if nent < ENT:
+            starts[nent] = True
+        prod = np.zeros(ENT)
+        for q, (g, v) in enumerate(entries):
+            prod[q] = v * vec[g]
+        pre = np.zeros(ENT)
+        for lane in range(32):
+            acc = 0.0
+            for j in range(IPT):
+                q = lane * IPT + j
+                acc = prod[q] + (0.0 if starts[q] else acc)
+                pre[val_slot(q)] = acc
+        for s, (a, b) in enumerate(zip(off[:-1], off[1:])):
+            total = 0.0
+            if a < b:
+                e = min((a | (IPT - 1)) + 1, b)
+                total = pre[val_slot(e - 1)]
+                while e < b:
+                    total += pre[val_slot(min(e + IPT, b) - 1)]
+                    e += IPT
+            out[first + s] = total
+    return out
+
+
+def emulate_hot(rp, ci, val, y, n, panels_max, vmax):
+    m = len(rp) - 1
+    lens = np.diff(rp)
+    thr = HOT_MIN_LEN
+    if m > vmax:
+        thr = max(thr, int(np.sort(lens)[::-1][vmax]) + 1)
+    hot = lens >= thr
+    hidx = np.cumsum(hot) - 1
+    hot_rows = np.nonzero(hot)[0]
+    assert len(hot_rows) <= vmax
+    width = (-(-n // panels_max) + 3) // 4 * 4
+    panels = -(-n // width)
+    # Aᵀ in column order, rows increasing within a column (the stored transpose)
+    cols = [[] for _ in range(panels * width)]
+    rest = np.zeros(n)
+    for i in range(m):
+        for k in range(rp[i], rp[i + 1]):
+            if hot[i]:
+                cols[ci[k]].append((int(hidx[i]), val[k]))
+            else:
+                rest[ci[k]] += val[k] * y[i]
+    assert max(len(c) for c in cols) <= ENT
+    vec = y[hot_rows]
+    part = np.full(panels * width, np.nan)
+    for p in range(panels):
+        segs = cols[p * width:(p + 1) * width]
+        recs = chunk_segments(segs)
+        assert sum(len(s) for _, s in recs) == width
+        part[p * width:(p + 1) * width] = run_records(recs, vec, width)
+    assert not np.isnan(part).any()
+    return part[:n] + rest, len(hot_rows)
+
+
+@pytest.mark.parametrize("seed,m,n,panels,vmax,a", [
+    (0, 500, 2000, 16, 40, 1.4),     # more long rows than the shared memory holds: the longest 40 or fewer
+    (1, 300, 700, 148, 1000, 1.4),   # narrow panels, every row of >= 32 entries hot
+    (2, 400, 5000, 8, 7, 1.8),       # few hot rows, wide panels, many empty column segments
+])
+def test_hot_part_of_transpose_product(seed, m, n, panels, vmax, a):
+    rng = np.random.default_rng(seed)
+    lengths = np.minimum(rng.zipf(a, size=m), n // 4)
+    rp, ci, val = _csr(m, n, rng, lengths)
+    y = rng.integers(-4, 5, size=m).astype(np.float64)
+    aty, nhot = emulate_hot(rp, ci, val, y, n, panels, vmax)
+    ref = np.zeros(n)
+    for i in range(m):
+        ref[ci[rp[i]:rp[i + 1]]] += val[rp[i]:rp[i + 1]] * y[i]
+    assert np.array_equal(aty, ref)
+    assert 0 < nhot <= vmax
