@@ -44,8 +44,9 @@ def test_struct_layouts_match_header():
     assert C.sizeof(L.CLp) == 4 * 4 + 8 + 8 * 8
     assert C.sizeof(L.COptions) == 8 + 4 * 8 + 8 + 4 * 6
     assert L.COptions.refine.offset == 36 and L.COptions.reserved_d.offset == 40
-    # persistent, gather_cache, launch_blocks, reserved[3] after reserved_d
+    # persistent, gather_cache, launch_blocks, panel_split, reserved[2] after reserved_d
     assert L.COptions.persistent.offset == 48 and L.COptions.launch_blocks.offset == 56
+    assert L.COptions.panel_split.offset == 60
     assert L.CResult.restarts.offset == 8 + 3 * 8 + 3 * 8
 
 
@@ -56,6 +57,7 @@ def test_default_options_match_reference(lib):
     assert o.tolerance == 1e-6 and o.max_iterations == 100000 and o.check_frequency == 100
     assert o.algorithm == 0 and o.termination == 0 and o.refine == 1
     assert o.persistent == 0 and o.gather_cache == 0 and o.launch_blocks == 0   # autotuned, automatic
+    assert o.panel_split == 0   # column-panel splits chosen automatically
     p = PdhgOptions()
     assert (p.tolerance, p.max_iterations, p.check_frequency) == (1e-6, 100000, 100)
 
