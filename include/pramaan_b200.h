@@ -128,7 +128,7 @@ typedef struct pramaan_pdhg_options {
                                  and not even that when gather_cache is 1 or
                                  -1: a fixed launch shape, for reproducible
                                  profiles                                       */
-    int32_t panel_split;      /* reference algorithm, the A x̄ product:
+    int32_t panel_split;      /* reference algorithm, the two products:
                                  0 (default): when rows of at least twice the
                                  panel count of entries hold half or more of
                                  A's non-zeros (power-law row lengths, at
@@ -138,7 +138,11 @@ typedef struct pramaan_pdhg_options {
                                  by the tiled product; 1: the same split
                                  whenever it is feasible; >= 2: the split with
                                  rows of at least that many entries as the long
-                                 rows; -1: the tiled product only.  Sums are
+                                 rows; -1: the tiled products only.  With A x̄
+                                 split, Aᵀy is split too where it can be: every
+                                 SM holds y of the longest rows of A and sums
+                                 their entries for its panel's columns, the
+                                 tiled product the other entries.  Sums are
                                  deterministic in every mode; a split changes
                                  the order of the additions within a row      */
     int32_t reserved[2];
