@@ -90,3 +90,35 @@ def test_two_ranks_solve_their_shards_and_gather_everything():
         owner = {i: r for r, p in enumerate(plan) for i in p}
         assert [x for _, x, _ in res] == [float(owner[i]) for i in range(len(nnz))]
         assert all(s == 0 for _, _, s in res)
+
+
+def test_shard_plan_with_iterations_equal_iterations_same_plan():
+    rng = np.random.default_rng(1)
+    nnz = list(rng.integers(0, 100000, size=61))
+    for world in (1, 2, 3, 8):
+        assert parallel.shard_plan(nnz, world, [5000.0] * 61) == parallel.shard_plan(nnz, world)
+
+
+def test_shard_plan_with_iterations_balances_the_slow_lps():
+    # rolling-horizon-like: many LPs of ~20-90 k iterations, a few of ~300 k, non-zeros
+    # unrelated to the iterations; the iteration-aware plan's modelled makespan is never
+    # worse than the non-zeros-only plan's, and better here
+    rng = np.random.default_rng(2)
+    n = 128
+    nnz = list(rng.integers(2_000, 90_000, size=n))
+    iters = list(rng.integers(20_000, 90_000, size=n).astype(float))
+    for k in rng.choice(n, 4, replace=False):
+        iters[k] = 300_000.0
+    for world in (2, 4, 8):
+        plan_it = parallel.shard_plan(nnz, world, iters)
+        plan_nz = parallel.shard_plan(nnz, world)
+        assert sorted(i for p in plan_it for i in p) == list(range(n))
+        assert plan_it == parallel.shard_plan(nnz, world, iters)     # deterministic
+        span_it = max(parallel.rank_seconds(nnz, iters, p) for p in plan_it)
+        span_nz = max(parallel.rank_seconds(nnz, iters, p) for p in plan_nz)
+        assert span_it <= span_nz * (1 + 1e-12)
+    assert span_it < span_nz
+    with pytest.raises(ValueError):
+        parallel.shard_plan([1, 2], 2, [1.0])
+    with pytest.raises(ValueError):
+        parallel.shard_plan([1, 2], 2, [1.0, -1.0])
