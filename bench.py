@@ -916,10 +916,13 @@ def run_gpu_arm(args):
                 "frac": achieved / hbm, "peak_kind": peak_kind,
                 "traffic": ncu_traffic(f"{tag}_zipf_lp_2Mx5M"),
                 "algorithmic_bytes_per_launch": kbytes, "avg_launch_ms": avg_s * 1000,
-                "timed_span": ("one product: its main kernel and its crossing-row completion kernel"
-                               if not (tag == "spmv_dual_fused" and panel["panels"]) else
-                               "one A x̄ product: the column-panel kernel of the long rows, the short rows' "
-                               "tiled product and its completion kernel, the long rows' finish kernel")}
+                "timed_span": ("one A x̄ product: the column-panel kernel of the long rows, the short rows' "
+                               "tiled product and its completion kernel, the long rows' finish kernel"
+                               if tag == "spmv_dual_fused" and panel["panels"] else
+                               "one Aᵀy product: the column-panel kernel of the hot rows, the tiled product of "
+                               "the other entries and its completion kernel"
+                               if tag == "spmv_primal_fused" and panel["primal_hot_rows"] else
+                               "one product: its main kernel and its crossing-row completion kernel")}
     other = [k for k in kinds if k[0] != tag][0]
     roofline["other_kernel"] = {"kernel": other[0], "achieved": other[2] / (other[1] / 1000 / args.steps) / 1e9,
                                 "frac": other[2] / (other[1] / 1000 / args.steps) / 1e9 / hbm,
